@@ -1,0 +1,49 @@
+/* Launch arguments of the integration kernels.
+ *
+ * One definition shared by the host library (C ABI) and the NVRTC-compiled
+ * device code, so the struct layout cannot drift between the two sides.
+ * Only pointer, 64-bit and 32-bit fields are used, in an order that needs
+ * no padding differences between compilers.
+ *
+ * Array layouts follow the reference (BatchSolverKernel.py:964-965 and
+ * output_sizes.py:284-380): the run index is the fastest axis, so
+ *   inits[k * run_stride + run], params[k * run_stride + run],
+ *   state_out[(row * width + k) * run_stride + run], and so on.
+ */
+#ifndef CBX_ARGS_H
+#define CBX_ARGS_H
+
+typedef struct cbx_solve_args {
+    /* inputs (device pointers, system precision) */
+    const void* inits;          /* [n_states][run_stride] */
+    const void* params;         /* [n_params][run_stride] */
+    const void* driver_coeffs;  /* [n_segments][n_drivers][order + 1] */
+    /* outputs (device pointers; NULL when the output is not compiled in) */
+    void* state_out;            /* [n_save_rows][n_saved_states + save_time][run_stride] */
+    void* obs_out;              /* [n_save_rows][n_saved_observables][run_stride] */
+    void* state_sum_out;        /* [n_summary_rows][n_summarised_states * per_var][run_stride] */
+    void* obs_sum_out;          /* [n_summary_rows][n_summarised_obs * per_var][run_stride] */
+    int* counters_out;          /* [n_save_rows][4][run_stride] int32 */
+    int* status_out;            /* [run_stride] int32 */
+    /* optional per-run arrays (NULL = uniform) */
+    const double* durations;    /* per-run integration duration */
+    const double* tol_scale;    /* per-run multiplier on every rtol */
+    /* scheduling and statistics */
+    unsigned long long* work_counter; /* persistent launch: next run to claim */
+    unsigned long long* totals;       /* [4]: steps, rejections, newton, krylov */
+    const volatile int* abort_flag;   /* host-visible abort request, or NULL */
+    /* sizes */
+    long long n_runs;
+    long long run_stride;
+    long long max_steps;        /* per-run step budget, 0 = unlimited */
+    /* timing (float64, as the reference's kernel scalars) */
+    double duration;
+    double warmup;
+    double t0;
+    double save_stop;
+    double summary_stop;
+    int n_save_rows;
+    int n_summary_rows;
+} cbx_solve_args;
+
+#endif /* CBX_ARGS_H */

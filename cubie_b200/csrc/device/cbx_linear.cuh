@@ -1,0 +1,342 @@
+// Matrix-free Krylov solvers for one system per thread.
+//
+// Each solver works on an operator object ``Op`` that provides
+//   static constexpr int K;                       // solver width
+//   void apply(const R* v, R* out) const;         // out = A v
+//   void precond(const R* v, R* out, R* scratch) const;  // out ~= A^-1 v
+//   C    wnorm2(const R* v) const;                // weighted mean-square norm
+//   C    tol(int i) const;                        // weight denominator of wnorm2
+// where wnorm2(v) = mean_i (|v_i| / tol(i))^2 is the reference's scaled
+// norm (src/cubie/integrators/norms.py:165-196) with the Krylov atol/rtol.
+//
+// Stopping rule of every solver: ||r|| <= floor + reduction * ||b|| in that
+// norm, fixed against the untouched right-hand side
+// (src/cubie/integrators/matrix_free_solvers/linear_solver.py:291-298).
+#pragma once
+#include "cbx_common.cuh"
+
+namespace cbx {
+
+// Preconditioned minimal-residual / steepest-descent iteration.
+// Follows MRLinearSolver (linear_solver.py:220-385): one operator and one
+// preconditioner application per iteration, x and r updated with
+// alpha = <t,r>/<t,t> (MR) or <r,z>/<t,z> (SD).  ``rhs`` is overwritten
+// with the running residual and ``x`` holds the initial guess on entry.
+template <class Cfg, class Op, bool SD>
+__device__ __forceinline__ int solve_mr(const Op& op, typename Cfg::R* rhs,
+                                        typename Cfg::R* x, int& iters) {
+    using R = typename Cfg::R;
+    using C = typename Cfg::C;
+    constexpr int K = Op::K;
+    const C rhs_norm2 = op.wnorm2(rhs);
+    const C tol = C(Cfg::KRYLOV_FLOOR) + C(Cfg::KRYLOV_REDUCTION) * sqrt_t(rhs_norm2);
+    const C tol2 = tol * tol;
+    R z[K];
+    R tmp[K];
+    op.apply(x, tmp);
+#pragma unroll
+    for (int i = 0; i < K; ++i) rhs[i] = rhs[i] - tmp[i];
+    C acc = op.wnorm2(rhs);
+    bool converged = acc <= tol2;
+    int it = 0;
+    for (int k = 0; k < Cfg::KRYLOV_MAX_ITERS; ++k) {
+        if (converged) break;
+        ++it;
+        if (Cfg::PRECONDITIONED) {
+            op.precond(rhs, z, tmp);
+        } else {
+#pragma unroll
+            for (int i = 0; i < K; ++i) z[i] = rhs[i];
+        }
+        op.apply(z, tmp);
+        C num = C(0), den = C(0);
+#pragma unroll
+        for (int i = 0; i < K; ++i) {
+            if (SD) {
+                num += C(rhs[i]) * C(z[i]);
+                den += C(tmp[i]) * C(z[i]);
+            } else {
+                num += C(tmp[i]) * C(rhs[i]);
+                den += C(tmp[i]) * C(tmp[i]);
+            }
+        }
+        const R alpha = (den != C(0)) ? R(num / den) : R(0);
+#pragma unroll
+        for (int i = 0; i < K; ++i) {
+            x[i] += alpha * z[i];
+            rhs[i] -= alpha * tmp[i];
+        }
+        acc = op.wnorm2(rhs);
+        converged = converged || (acc <= tol2);
+    }
+    iters = it;
+    return converged ? SUCCESS : MAX_LINEAR_ITERATIONS_EXCEEDED;
+}
+
+template <class R> __device__ __forceinline__ R clampd(R v, R lim) {
+    v = (v > lim) ? lim : v;
+    return (v < -lim) ? -lim : v;
+}
+
+// Preconditioned BiCGSTAB with the reference's breakdown and overflow
+// guards (bicgstab_solver.py:367-663): clamps every vector element and
+// product to +-dot_clamp, flags BICGSTAB_BREAKDOWN when rho or omega
+// collapse (1e-30 in float32, 1e-200 in float64) or a recurrence quotient
+// would leave the clamp budget.
+template <class Cfg, class Op>
+__device__ __forceinline__ int solve_bicgstab(const Op& op, typename Cfg::R* rhs,
+                                              typename Cfg::R* x, int& iters) {
+    using R = typename Cfg::R;
+    using C = typename Cfg::C;
+    constexpr int K = Op::K;
+    constexpr bool F32 = sizeof(R) == 4;
+    const R tiny = F32 ? R(1e-30) : R(1e-200);
+    const R lim = F32 ? R(1e16) : R(1e150);
+    R r0[K], p[K], v[K], tmp[K], sh[K];
+
+    const C rhs_norm2 = op.wnorm2(rhs);
+    const C tol = C(Cfg::KRYLOV_FLOOR) + C(Cfg::KRYLOV_REDUCTION) * sqrt_t(rhs_norm2);
+    const C tol2 = tol * tol;
+    op.apply(x, tmp);
+    R rho_prev = R(0);
+#pragma unroll
+    for (int i = 0; i < K; ++i) {
+        const R ax = clampd(tmp[i], lim);
+        const R ri = rhs[i] - ax;
+        rhs[i] = ri;
+        r0[i] = ri;
+        p[i] = clampd(ri, lim);
+        R sq = ri * ri;
+        sq = (sq > lim) ? lim : sq;
+        rho_prev += sq;
+    }
+    C acc = op.wnorm2(rhs);
+    bool converged = acc <= tol2;
+    bool broken = false;
+    bool finished = converged;
+    int it = 0;
+    for (int k = 0; k < Cfg::KRYLOV_MAX_ITERS; ++k) {
+        if (finished) break;
+        ++it;
+        if (Cfg::PRECONDITIONED) {
+            op.precond(p, tmp, v);
+#pragma unroll
+            for (int i = 0; i < K; ++i) tmp[i] = clampd(tmp[i], lim);
+        } else {
+#pragma unroll
+            for (int i = 0; i < K; ++i) tmp[i] = p[i];
+        }
+        op.apply(tmp, v);
+        R dot_r0v = R(0);
+#pragma unroll
+        for (int i = 0; i < K; ++i) {
+            v[i] = clampd(v[i], lim);
+            dot_r0v += clampd(r0[i] * v[i], lim);
+        }
+        const bool alpha_overflow = absv(rho_prev) > absv(dot_r0v) * lim;
+        broken = broken || alpha_overflow;
+        finished = converged || broken;
+        const R alpha = (dot_r0v != R(0) && !alpha_overflow) ? rho_prev / dot_r0v : R(0);
+        const R alpha_eff = finished ? R(0) : alpha;
+#pragma unroll
+        for (int i = 0; i < K; ++i) {
+            x[i] = x[i] + alpha_eff * tmp[i];
+            rhs[i] = rhs[i] - alpha_eff * v[i];
+        }
+        acc = op.wnorm2(rhs);
+        converged = converged || (acc <= tol2);
+        finished = converged || broken;
+        if (Cfg::PRECONDITIONED) {
+            op.precond(rhs, sh, tmp);
+#pragma unroll
+            for (int i = 0; i < K; ++i) sh[i] = clampd(sh[i], lim);
+        } else {
+#pragma unroll
+            for (int i = 0; i < K; ++i) sh[i] = clampd(rhs[i], lim);
+        }
+        op.apply(sh, tmp);
+        R dot_ts = R(0), dot_tt = R(0);
+#pragma unroll
+        for (int i = 0; i < K; ++i) {
+            tmp[i] = clampd(tmp[i], lim);
+            dot_ts += clampd(tmp[i] * rhs[i], lim);
+            R sq = tmp[i] * tmp[i];
+            dot_tt += (sq > lim) ? lim : sq;
+        }
+        const bool omega_overflow = absv(dot_ts) > dot_tt * lim;
+        const R omega = (dot_tt != R(0) && !omega_overflow) ? dot_ts / dot_tt : R(0);
+        const R omega_eff = finished ? R(0) : omega;
+#pragma unroll
+        for (int i = 0; i < K; ++i) {
+            x[i] = x[i] + omega_eff * sh[i];
+            rhs[i] = rhs[i] - omega_eff * tmp[i];
+        }
+        acc = op.wnorm2(rhs);
+        converged = converged || (acc <= tol2);
+        R rho_new = R(0);
+#pragma unroll
+        for (int i = 0; i < K; ++i) rho_new += clampd(r0[i] * rhs[i], lim);
+        const bool rho_bad = absv(rho_new) < tiny;
+        const bool omega_bad = absv(omega) < tiny;
+        broken = broken || (!converged && (rho_bad || omega_bad));
+        finished = converged || broken;
+        const bool beta_overflow = (absv(rho_new) > absv(rho_prev) * lim) ||
+                                   (absv(alpha) > absv(omega) * lim);
+        broken = broken || (!finished && beta_overflow);
+        finished = converged || broken;
+        const R beta = !finished ? (rho_new / rho_prev) * (alpha / omega) : R(0);
+#pragma unroll
+        for (int i = 0; i < K; ++i) {
+            R pi = !finished ? rhs[i] + beta * (p[i] - omega * v[i]) : p[i];
+            p[i] = clampd(pi, lim);
+        }
+        rho_prev = !finished ? rho_new : rho_prev;
+    }
+    iters = it;
+    if (converged) return SUCCESS;
+    return broken ? BICGSTAB_BREAKDOWN : MAX_LINEAR_ITERATIONS_EXCEEDED;
+}
+
+// Restarted GMRES(m) with right preconditioning and modified Gram-Schmidt.
+//
+// There is no GMRES in the reference; this solver uses its stopping rule.
+// The system is scaled by W = diag(1 / (tol_i sqrt(K))), so the 2-norm of
+// the scaled residual equals the reference's weighted RMS norm and the
+// Givens-rotated residual estimate |g_{j+1}| is checked directly against
+// floor + reduction * ||b||.  Basis vectors are stored in R, inner
+// products, the Hessenberg matrix and rotations in C (FP64 in mixed
+// precision).  One Arnoldi step (one operator and one preconditioner
+// application) counts as one iteration.
+template <class Cfg, class Op>
+__device__ __forceinline__ int solve_gmres(const Op& op, typename Cfg::R* rhs,
+                                           typename Cfg::R* x, int& iters) {
+    using R = typename Cfg::R;
+    using C = typename Cfg::C;
+    constexpr int K = Op::K;
+    constexpr int M = (Cfg::GMRES_RESTART < K) ? Cfg::GMRES_RESTART : K;
+    R V[M + 1][K];
+    C H[M][M];
+    C g[M + 1], cs[M], sn[M], yv[M];
+    R b[K], w[K], z[K];
+    const C sK = sqrt_t(C(K));
+
+    const C rhs_norm2 = op.wnorm2(rhs);
+    const C tol = C(Cfg::KRYLOV_FLOOR) + C(Cfg::KRYLOV_REDUCTION) * sqrt_t(rhs_norm2);
+    op.apply(x, w);
+#pragma unroll
+    for (int i = 0; i < K; ++i) {
+        b[i] = rhs[i];
+        rhs[i] = rhs[i] - w[i];
+    }
+    C beta = sqrt_t(op.wnorm2(rhs));
+    bool converged = beta <= tol;
+    int it = 0;
+    while (!converged && it < Cfg::KRYLOV_MAX_ITERS) {
+        const C inv_beta = C(1) / beta;
+#pragma unroll
+        for (int i = 0; i < K; ++i) V[0][i] = R(C(rhs[i]) / (op.tol(i) * sK) * inv_beta);
+        g[0] = beta;
+#pragma unroll
+        for (int j = 1; j <= M; ++j) g[j] = C(0);
+        int jend = 0;
+#pragma unroll
+        for (int j = 0; j < M; ++j) {
+            if (it >= Cfg::KRYLOV_MAX_ITERS) break;
+            ++it;
+            // z = P^-1 W^-1 V_j ; w = W A z
+#pragma unroll
+            for (int i = 0; i < K; ++i) w[i] = R(C(V[j][i]) * op.tol(i) * sK);
+            if (Cfg::PRECONDITIONED) {
+                op.precond(w, z, V[M]);
+            } else {
+#pragma unroll
+                for (int i = 0; i < K; ++i) z[i] = w[i];
+            }
+            op.apply(z, w);
+#pragma unroll
+            for (int i = 0; i < K; ++i) w[i] = R(C(w[i]) / (op.tol(i) * sK));
+            C hcol[M + 1];
+#pragma unroll
+            for (int l = 0; l < M; ++l) {
+                if (l <= j) {
+                    C dot = C(0);
+#pragma unroll
+                    for (int i = 0; i < K; ++i) dot += C(w[i]) * C(V[l][i]);
+                    hcol[l] = dot;
+#pragma unroll
+                    for (int i = 0; i < K; ++i) w[i] = R(C(w[i]) - dot * C(V[l][i]));
+                }
+            }
+            C hn = C(0);
+#pragma unroll
+            for (int i = 0; i < K; ++i) hn += C(w[i]) * C(w[i]);
+            hn = sqrt_t(hn);
+            {
+                const C inv = (hn > C(0)) ? C(1) / hn : C(0);
+#pragma unroll
+                for (int i = 0; i < K; ++i) V[j + 1][i] = R(C(w[i]) * inv);
+            }
+#pragma unroll
+            for (int l = 0; l < M - 1; ++l) {
+                if (l < j) {
+                    const C a0 = hcol[l], a1 = hcol[l + 1];
+                    hcol[l] = cs[l] * a0 + sn[l] * a1;
+                    hcol[l + 1] = -sn[l] * a0 + cs[l] * a1;
+                }
+            }
+            const C a = hcol[j];
+            const C den = sqrt_t(a * a + hn * hn);
+            const C c = (den > C(0)) ? a / den : C(1);
+            const C s = (den > C(0)) ? hn / den : C(0);
+            cs[j] = c;
+            sn[j] = s;
+            hcol[j] = den;
+            g[j + 1] = -s * g[j];
+            g[j] = c * g[j];
+#pragma unroll
+            for (int l = 0; l < M; ++l)
+                if (l <= j) H[l][j] = hcol[l];
+            jend = j + 1;
+            if (absv(g[j + 1]) <= tol || hn == C(0)) break;
+        }
+        if (jend == 0) break;
+        // back substitution H y = g on the leading jend x jend block
+#pragma unroll
+        for (int l = M - 1; l >= 0; --l) {
+            if (l < jend) {
+                C s = g[l];
+#pragma unroll
+                for (int m = 0; m < M; ++m)
+                    if (m > l && m < jend) s -= H[l][m] * yv[m];
+                yv[l] = (H[l][l] != C(0)) ? s / H[l][l] : C(0);
+            }
+        }
+        // x += P^-1 W^-1 sum_l y_l V_l
+#pragma unroll
+        for (int i = 0; i < K; ++i) {
+            C u = C(0);
+#pragma unroll
+            for (int l = 0; l < M; ++l)
+                if (l < jend) u += yv[l] * C(V[l][i]);
+            w[i] = R(u * op.tol(i) * sK);
+        }
+        if (Cfg::PRECONDITIONED) {
+            op.precond(w, z, V[M]);
+        } else {
+#pragma unroll
+            for (int i = 0; i < K; ++i) z[i] = w[i];
+        }
+#pragma unroll
+        for (int i = 0; i < K; ++i) x[i] += z[i];
+        // true residual decides convergence
+        op.apply(x, w);
+#pragma unroll
+        for (int i = 0; i < K; ++i) rhs[i] = b[i] - w[i];
+        beta = sqrt_t(op.wnorm2(rhs));
+        converged = beta <= tol;
+    }
+    iters = it;
+    return converged ? SUCCESS : MAX_LINEAR_ITERATIONS_EXCEEDED;
+}
+
+}  // namespace cbx

@@ -1,0 +1,104 @@
+/* cubie_b200 C ABI: compile, load and launch batch ODE integration kernels.
+ *
+ * The reference (ccam80/cubie) has no native boundary: its Python
+ * BatchSolverKernel.run (src/cubie/batchsolving/BatchSolverKernel.py:525-604)
+ * JIT-compiles one Numba kernel per configuration (build_kernel, :851-1011)
+ * and launches it once per chunk (_execute_run, :741-762).  This library is
+ * the seam that call now crosses: the Python layer (or any other host)
+ * generates CUDA C++ for a configuration, compiles it here with NVRTC for
+ * sm_100a, and launches the plain or persistent integration kernel with
+ * caller-owned device buffers.
+ *
+ * Conventions: every function returns 0 on success and a negative code on
+ * failure; cbx_last_error() then describes the failure for the calling
+ * thread.  The library never frees caller memory.  Streams are CUstream /
+ * cudaStream_t handles passed as void*.
+ */
+#ifndef CUBIE_B200_H
+#define CUBIE_B200_H
+
+#include <stddef.h>
+#include "../cubie_b200/csrc/device/cbx_args.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct cbx_module cbx_module;
+
+enum cbx_kernel_kind { CBX_KERNEL_PLAIN = 0, CBX_KERNEL_PERSISTENT = 1 };
+
+enum cbx_error {
+    CBX_OK = 0,
+    CBX_ERR_ARGUMENT = -1,
+    CBX_ERR_NVRTC = -2,
+    CBX_ERR_DRIVER = -3,
+    CBX_ERR_RUNTIME = -4,
+    CBX_ERR_NO_DEVICE = -5
+};
+
+/* Library version (major * 10000 + minor * 100 + patch). */
+int cbx_version(void);
+
+/* Thread-local description of the last failure (replaces the Python
+ * exceptions the reference raises, e.g. limit_blocksize's ValueError,
+ * BatchSolverKernel.py:823-830). */
+const char* cbx_last_error(void);
+
+/* NVRTC version linked into the library. */
+int cbx_nvrtc_version(int* major, int* minor);
+
+/* Compile CUDA C++ source to an sm_100a cubin with NVRTC.  No GPU needed.
+ * *cubin is malloc'ed; release it with cbx_free.  ``log`` receives the
+ * compiler log (truncated to log_len, always NUL-terminated when
+ * log_len > 0).  Replaces the Numba compile that reading
+ * BatchSolverKernel.kernel triggers (CUDAFactory.get_cached_output). */
+int cbx_compile(const char* source, const char* name, const char* const* options, int n_options,
+                void** cubin, size_t* cubin_size, char* log, size_t log_len);
+void cbx_free(void* p);
+
+/* Load a cubin on ``device`` (primary context) and resolve the
+ * integration kernels cbx_integrate_plain and cbx_integrate_persistent. */
+int cbx_module_load(const void* cubin, size_t cubin_size, int device, cbx_module** module);
+
+/* cbx_compile + cbx_module_load. */
+int cbx_module_create(const char* source, const char* const* options, int n_options, int device,
+                      cbx_module** module, char* log, size_t log_len);
+
+int cbx_module_destroy(cbx_module* module);
+
+/* Resource use of a kernel (registers per thread, local bytes per thread,
+ * max threads per block, static shared bytes). */
+int cbx_kernel_info(cbx_module* module, int kernel, int* registers, int* local_bytes,
+                    int* max_threads, int* shared_bytes);
+
+/* Resident blocks per SM for ``block`` threads. */
+int cbx_occupancy(cbx_module* module, int kernel, int block, int* blocks_per_sm);
+
+/* Launch the integration kernel: the replacement for the reference's
+ * kernel launch (BatchSolverKernel.py:741-762).  ``args`` holds caller
+ * device pointers (layouts in cbx_args.h).  grid = 0 picks
+ * ceil(n_runs / block) for the plain kernel and a resident grid for the
+ * persistent kernel (which also requires args->work_counter to point at a
+ * zeroed device counter).  Asynchronous on ``stream``. */
+int cbx_solve(cbx_module* module, const cbx_solve_args* args, int kernel, int block, int grid,
+              void* stream);
+
+/* Device facts used for launch geometry. */
+int cbx_device_info(int device, int* sm_count, int* cc_major, int* cc_minor);
+
+/* FP32 fused multiply-add throughput probe: launches a fixed FMA loop
+ * (nvcc-compiled for sm_100a) and returns the elapsed milliseconds for
+ * ``flops`` floating-point operations.  Used to state the FP32 roofline
+ * denominator next to the integrator's achieved FLOP rate. */
+int cbx_fp32_peak_probe(int device, double* flops, float* milliseconds);
+
+/* Overwrite ``bytes`` of device memory at ``buffer`` on ``stream`` (L2
+ * flush between timed launches). */
+int cbx_flush_l2(void* buffer, size_t bytes, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CUBIE_B200_H */

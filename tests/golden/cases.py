@@ -1,0 +1,117 @@
+"""Seeded parity cases shared by the fixture generator and the tests.
+
+Every case names a system (equation strings), an algorithm alias, the
+solver keywords, the integration window and how its seeded inputs are
+drawn.  ``make_reference_fixtures.py`` runs each case through the
+reference's own kernels (CPU, Numba CUDA simulator) and stores the outputs
+as ``ref_<name>.npz``; the tests run the same case through the oracle and
+through the CUDA engine.
+"""
+
+import numpy as np
+
+LORENZ = dict(
+    equations=["dx = sigma * (y - x)", "dy = x * (rho - z) - y", "dz = x * y - beta * z"],
+    states=["x", "y", "z"], parameters=["rho"], constants={"sigma": 10.0, "beta": 8.0 / 3.0},
+)
+VDP = dict(
+    equations=["dx = y", "dy = mu * (1 - x**2) * y - x"],
+    states=["x", "y"], parameters=["mu"], constants={},
+)
+FHN = dict(
+    equations=["dV = V - V**3 / 3 - w + I", "dw = (V + a - b * w) / tau"],
+    states=["V", "w"], parameters=["a", "b", "tau", "I"], constants={},
+)
+
+
+def lorenz_inputs(n, seed):
+    rng = np.random.default_rng(seed)
+    rho = rng.uniform(20.0, 35.0, n)
+    x0 = rng.uniform(-10.0, 10.0, (3, n))
+    return x0, rho[None, :]
+
+
+def vdp_inputs(n, seed, mus):
+    rng = np.random.default_rng(seed)
+    x0 = rng.uniform(-2.0, 2.0, (2, n))
+    return x0, np.asarray(mus, dtype=float)[None, :]
+
+
+def fhn_inputs(n, seed):
+    rng = np.random.default_rng(seed)
+    p = np.stack([rng.uniform(0.5, 0.9, n), rng.uniform(0.6, 1.0, n), rng.uniform(8.0, 15.0, n),
+                  rng.uniform(0.3, 0.6, n)])
+    x0 = np.stack([rng.uniform(-1.0, 1.0, n), rng.uniform(-0.5, 0.5, n)])
+    return x0, p
+
+
+CASES = {
+    "lorenz_dp54_f32": dict(system=LORENZ, algorithm="dormand-prince-54", precision="float32",
+                            inputs=("lorenz", 8, 1), duration=1.0,
+                            kwargs=dict(rtol=1e-6, atol=1e-8, save_every=0.05, summarise_every=0.25,
+                                        sample_summaries_every=0.05,
+                                        output_types=["state", "time", "iteration_counters", "mean", "max"])),
+    "lorenz_dp54_f64": dict(system=LORENZ, algorithm="dormand-prince-54", precision="float64",
+                            inputs=("lorenz", 8, 1), duration=1.0,
+                            kwargs=dict(rtol=1e-8, atol=1e-10, save_every=0.05, summarise_every=0.25,
+                                        sample_summaries_every=0.05,
+                                        output_types=["state", "time", "iteration_counters", "mean", "max"])),
+    "lorenz_dp54_pid_f64": dict(system=LORENZ, algorithm="dormand-prince-54", precision="float64",
+                                inputs=("lorenz", 4, 2), duration=0.5,
+                                kwargs=dict(rtol=1e-7, atol=1e-9, save_every=0.1, step_controller="pid",
+                                            kp=0.7, ki=-0.4, kd=0.1, output_types=["state", "time"])),
+    "lorenz_dp54_i_f64": dict(system=LORENZ, algorithm="dormand-prince-54", precision="float64",
+                              inputs=("lorenz", 4, 3), duration=0.5,
+                              kwargs=dict(rtol=1e-7, atol=1e-9, save_every=0.1, step_controller="i",
+                                          output_types=["state", "time"])),
+    "lorenz_dp54_gus_f64": dict(system=LORENZ, algorithm="dormand-prince-54", precision="float64",
+                                inputs=("lorenz", 4, 4), duration=0.5,
+                                kwargs=dict(rtol=1e-7, atol=1e-9, save_every=0.1, step_controller="gustafsson",
+                                            output_types=["state", "time"])),
+    "vdp_ros3p_f32": dict(system=VDP, algorithm="ros3p", precision="float32",
+                          inputs=("vdp", 4, 5, [1.0, 3.0, 10.0, 30.0]), duration=2.0,
+                          kwargs=dict(rtol=1e-6, atol=1e-6, save_every=0.25,
+                                      output_types=["state", "time", "iteration_counters"])),
+    "vdp_ros3p_bicgstab_f64": dict(system=VDP, algorithm="ros3p", precision="float64",
+                                   inputs=("vdp", 4, 6, [1.0, 3.0, 10.0, 30.0]), duration=2.0,
+                                   kwargs=dict(rtol=1e-7, atol=1e-7, save_every=0.25,
+                                               linear_correction_type="bicgstab",
+                                               output_types=["state", "time", "iteration_counters"])),
+    "vdp_radau_f32": dict(system=VDP, algorithm="radau", precision="float32",
+                          inputs=("vdp", 2, 7, [2.0, 20.0]), duration=0.5,
+                          kwargs=dict(rtol=1e-6, atol=1e-6, save_every=0.125,
+                                      output_types=["state", "time", "iteration_counters"])),
+    "vdp_radau_f64": dict(system=VDP, algorithm="radau", precision="float64",
+                          inputs=("vdp", 2, 8, [2.0, 20.0]), duration=0.5,
+                          kwargs=dict(rtol=1e-8, atol=1e-8, save_every=0.125,
+                                      output_types=["state", "time", "iteration_counters"])),
+    "vdp_dirk3_bicgstab_f32": dict(system=VDP, algorithm="l_stable_dirk_3", precision="float32",
+                                   inputs=("vdp", 2, 9, [2.0, 10.0]), duration=0.5,
+                                   kwargs=dict(dt=0.01, rtol=1e-6, atol=1e-6, save_every=0.125,
+                                               linear_correction_type="bicgstab",
+                                               output_types=["state", "time", "iteration_counters"])),
+    "vdp_sdirk4_f64": dict(system=VDP, algorithm="l_stable_sdirk_4", precision="float64",
+                           inputs=("vdp", 2, 10, [2.0, 10.0]), duration=0.5,
+                           kwargs=dict(rtol=1e-7, atol=1e-7, save_every=0.125,
+                                       output_types=["state", "time", "iteration_counters"])),
+    "fhn_dp54_peaks_f32": dict(system=FHN, algorithm="dormand-prince-54", precision="float32",
+                               inputs=("fhn", 4, 11), duration=40.0,
+                               kwargs=dict(rtol=1e-6, atol=1e-6, save_every=1.0, summarise_every=20.0,
+                                           sample_summaries_every=0.5,
+                                           output_types=["state", "time", "peaks[3]", "std", "rms", "min"])),
+    "lorenz_step_too_small_f32": dict(system=LORENZ, algorithm="dormand-prince-54", precision="float32",
+                                      inputs=("lorenz", 2, 12), duration=1.0,
+                                      kwargs=dict(rtol=1e-12, atol=1e-14, dt=0.01, dt_min=0.005, dt_max=0.1,
+                                                  output_types=["state", "time"])),
+}
+
+
+def case_inputs(case):
+    kind = case["inputs"][0]
+    if kind == "lorenz":
+        return lorenz_inputs(case["inputs"][1], case["inputs"][2])
+    if kind == "vdp":
+        return vdp_inputs(case["inputs"][1], case["inputs"][2], case["inputs"][3])
+    if kind == "fhn":
+        return fhn_inputs(case["inputs"][1], case["inputs"][2])
+    raise KeyError(kind)

@@ -1,0 +1,32 @@
+"""Helpers shared by the parity tests."""
+
+import numpy as np
+
+from cases import CASES, case_inputs
+
+
+def build_case_system(case):
+    from cubie_b200 import create_ODE_system
+    sd = case["system"]
+    prec = np.dtype(case["precision"]).type
+    return create_ODE_system(sd["equations"], states={s: 0.0 for s in sd["states"]},
+                             parameters={p: 0.0 for p in sd["parameters"]}, constants=sd["constants"],
+                             precision=prec, strict=True)
+
+
+def run_oracle(case, **overrides):
+    from oracle import OracleSystem, integrate
+    sd = case["system"]
+    osys = OracleSystem(sd["equations"], sd["states"], sd["parameters"], sd["constants"])
+    inits, params = case_inputs(case)
+    kw = dict(case["kwargs"])
+    kw["precision"] = np.dtype(case["precision"]).type
+    kw.update(overrides)
+    return integrate(osys, case["algorithm"], inits, params, case["duration"], **kw)
+
+
+def tol_units(a, b, atol, rtol):
+    """|a - b| in units of atol + rtol |b| (NaN-safe max)."""
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    return float(np.nanmax(np.abs(a - b) / (atol + rtol * np.abs(b)))) if a.size else 0.0

@@ -1,0 +1,74 @@
+"""Pin the CPU oracle to the reference's own outputs (no GPU).
+
+The fixtures ``tests/golden/ref_*.npz`` were produced by running the
+unmodified reference kernels on the CPU (Numba CUDA simulator) through
+``tests/golden/make_reference_fixtures.py``.  In float64 the oracle must
+reproduce them to a small fraction of the tolerance envelope with the same
+step and rejection counts; in float32 the reference compiles with fast-math
+(approximate division and transcendentals), so rounding paths differ and
+agreement is judged in tolerance units on non-chaotic cases.
+"""
+
+import json
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from cases import CASES
+from parity_utils import run_oracle, tol_units
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+
+F64_CASES = [n for n, c in CASES.items() if c["precision"] == "float64"]
+F32_CASES = [n for n, c in CASES.items() if c["precision"] == "float32"]
+
+
+def _load(name):
+    path = GOLDEN / f"ref_{name}.npz"
+    if not path.exists():
+        pytest.fail(f"missing fixture {path.name}; run tests/golden/make_reference_fixtures.py")
+    return np.load(path)
+
+
+@pytest.mark.parametrize("name", F64_CASES)
+def test_oracle_matches_reference_float64(name):
+    case = CASES[name]
+    ref = _load(name)
+    out = run_oracle(case)
+    kw = case["kwargs"]
+    assert out["status"].tolist() == ref["status"].tolist()
+    assert out["state"].shape == ref["state"].shape
+    assert tol_units(out["state"], ref["state"], kw["atol"], kw["rtol"]) < 1e-3
+    if "iteration_counters" in ref.files:
+        np.testing.assert_array_equal(out["iteration_counters"][:, 2:, :], ref["iteration_counters"][:, 2:, :])
+    if "state_summaries" in ref.files:
+        assert tol_units(out["state_summaries"], ref["state_summaries"], kw["atol"], kw["rtol"]) < 1e-3
+
+
+@pytest.mark.parametrize("name", F32_CASES)
+def test_oracle_matches_reference_float32(name):
+    case = CASES[name]
+    ref = _load(name)
+    out = run_oracle(case)
+    kw = case["kwargs"]
+    assert out["status"].tolist() == ref["status"].tolist()
+    assert out["state"].shape == ref["state"].shape
+    if name.startswith("lorenz_dp54"):
+        # chaotic: float32 rounding differences grow like exp(0.9 t); compare
+        # the first fifth of the window and the run-level step counts
+        k = max(2, ref["state"].shape[0] // 5)
+        assert tol_units(out["state"][:k], ref["state"][:k], 1e-6, 1e-5) < 10
+        steps_o = out["iteration_counters"][:, 2, :].sum(0)
+        steps_r = ref["iteration_counters"][:, 2, :].sum(0)
+        assert np.all(np.abs(steps_o - steps_r) <= 2)
+    else:
+        assert tol_units(out["state"], ref["state"], kw["atol"], kw["rtol"]) < 10
+    if "state_summaries" in ref.files and not name.startswith("lorenz"):
+        assert tol_units(out["state_summaries"], ref["state_summaries"], kw["atol"], kw["rtol"]) < 10
+
+
+def test_fixture_summary_legends_present():
+    ref = _load("fhn_dp54_peaks_f32")
+    legend = json.loads(str(ref["summaries_legend"]))
+    assert any("peaks" in v for v in legend.values())
