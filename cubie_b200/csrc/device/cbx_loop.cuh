@@ -212,16 +212,20 @@ __device__ __forceinline__ bool lane_iterate(Lane<Cfg>& L, const cbx_solve_args 
         at_end = (L.tp < L.t_end) && finished;
         finished = finished && !at_end;
     }
-    if (a.max_steps > 0 && L.steps >= a.max_steps && !finished) {
+    finished = finished || L.irrecoverable;
+    if (finished) return true;
+    // Step budget and host abort request end the run with status bit 32
+    // (reserved but unused in the reference, result_codes.py:57).  Written
+    // as direct returns: folding them into ``irrecoverable`` ahead of the
+    // finish test made NVRTC's optimiser drop the event clamp below.
+    if (a.max_steps > 0 && L.steps >= a.max_steps) {
         L.status |= MAX_LOOP_ITERS_EXCEEDED;
-        L.irrecoverable = true;
+        return true;
     }
     if (a.abort_flag && (L.steps & 255) == 0 && *a.abort_flag) {
         L.status |= MAX_LOOP_ITERS_EXCEEDED;
-        L.irrecoverable = true;
+        return true;
     }
-    finished = finished || L.irrecoverable;
-    if (finished) return true;
 
     bool do_save = Cfg::SAVE_REG ? ((end_of_step >= L.next_save) && !save_finished) : false;
     bool do_update = Cfg::SUMM_REG ? ((end_of_step >= L.next_update) && !summary_finished) : false;

@@ -440,8 +440,9 @@ class Solver:
                         block=blocksize)
 
     def prepare(self, duration: float, settling_time: float = 0.0, t0: float = 0.0,
-                interp=None, durations=None) -> Dict[str, Any]:
-        """Compile the module and compute output sizes for a launch."""
+                interp=None, durations=None, load: bool = True) -> Dict[str, Any]:
+        """Compile (and with ``load``, load) the module and compute output
+        sizes for a launch."""
         if duration <= 0:
             raise ValueError("duration must be positive")
         timing = self._timing(float(duration))
@@ -449,7 +450,10 @@ class Solver:
             raise ValueError("per-run durations need end-of-run saving only (no save_every or summaries)")
         driver_meta = interp.device_meta() if interp is not None else None
         spec = self.kernel_spec(timing, driver_meta)
-        mod, gk = self.module_for(spec)
+        if load:
+            mod, gk = self.module_for(spec)
+        else:
+            mod, gk = None, generate_kernel(self.system, spec)
         p = self.precision
         n_save = output_length(duration, timing["save_every"], timing["save_last"], p) if timing["time_domain"] else 0
         n_summ = summaries_length(duration, timing["sample_every"], timing["samples_per_summary"], p) \

@@ -1,0 +1,117 @@
+"""Run a generated integrator translation unit on the CPU (test harness).
+
+The generated CUDA source is compiled by g++ with ``cbx_host_emu.h`` forced
+in front, plus a small driver that loops over (block, thread) and calls the
+kernel body for each emulated thread.  Inputs and outputs are numpy arrays
+whose pointers go into the same ``cbx_solve_args`` struct the GPU launch
+uses.
+"""
+
+import ctypes
+import hashlib
+import os
+import subprocess
+import tempfile
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ROOT = HERE.parent.parent
+DEVICE = ROOT / "cubie_b200" / "csrc" / "device"
+
+DRIVER = r"""
+cbx_dim3 threadIdx, blockIdx, blockDim, gridDim;
+extern "C" void emu_launch(cbx_solve_args* a, int kernel, int grid, int block) {
+    blockDim = {(unsigned)block, 1, 1};
+    gridDim = {(unsigned)grid, 1, 1};
+    for (int b = 0; b < grid; ++b) {
+        for (int t = 0; t < block; ++t) {
+            blockIdx = {(unsigned)b, 0, 0};
+            threadIdx = {(unsigned)t, 0, 0};
+            if (kernel == 0) cbx_integrate_plain(*a);
+            else cbx_integrate_persistent(*a);
+        }
+    }
+}
+"""
+
+_cache = {}
+
+
+def compile_emulated(source: str):
+    key = hashlib.sha256((source + (HERE / "cbx_host_emu.h").read_text()).encode()).hexdigest()[:20]
+    if key in _cache:
+        return _cache[key]
+    d = Path(tempfile.gettempdir()) / "cbx_emu"
+    d.mkdir(exist_ok=True)
+    src = d / f"{key}.cpp"
+    so = d / f"{key}.so"
+    if not so.exists():
+        src.write_text(source + DRIVER)
+        cmd = ["g++", "-O1", "-std=c++17", "-shared", "-fPIC", "-include", str(HERE / "cbx_host_emu.h"),
+               f"-I{DEVICE}", "-x", "c++", str(src), "-o", str(so)]
+        subprocess.run(cmd, check=True, capture_output=True, text=True)
+    lib = ctypes.CDLL(str(so))
+    lib.emu_launch.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    _cache[key] = lib
+    return lib
+
+
+def run_emulated(solver, inits, params, duration, settling_time=0.0, t0=0.0, kernel="plain",
+                 durations=None, tol_scale=None):
+    """Integrate with the solver's generated kernel on the CPU; returns a dict
+    of output arrays laid out like ``SolveResult``."""
+    from cubie_b200 import _native
+    prep = solver.prepare(duration, settling_time, t0, None, durations, load=False)
+    spec = prep["spec"]
+    gk = prep["gen"]
+    lib = compile_emulated(gk.source)
+    p = solver.precision
+    n_runs = inits.shape[1]
+    inits = np.ascontiguousarray(inits, dtype=p)
+    params = np.ascontiguousarray(params, dtype=p) if params.size else np.zeros((1, n_runs), p)
+    n_save, n_summ = prep["n_save"], prep["n_summ"]
+    width = (len(spec.saved_state_indices) if spec.save_state else 0) + (1 if spec.save_time else 0)
+    per_var = spec.summary.output_per_var if spec.summary else 0
+    bufs = {
+        "state": np.zeros((n_save, width, n_runs), p) if width else None,
+        "obs": np.zeros((n_save, len(spec.saved_observable_indices), n_runs), p) if spec.save_observables else None,
+        "state_sum": np.zeros((n_summ, len(spec.summarised_state_indices) * per_var, n_runs), p)
+        if spec.summarised_state_indices and per_var else None,
+        "obs_sum": np.zeros((n_summ, len(spec.summarised_observable_indices) * per_var, n_runs), p)
+        if spec.summarised_observable_indices and per_var else None,
+        "counters": np.zeros((n_save, 4, n_runs), np.int32) if spec.save_counters else None,
+        "status": np.zeros((n_runs,), np.int32),
+        "work": np.zeros((2,), np.int64),
+        "totals": np.zeros((4,), np.int64),
+    }
+    dur = np.ascontiguousarray(durations, dtype=np.float64) if durations is not None else None
+    tsc = np.ascontiguousarray(tol_scale, dtype=np.float64) if tol_scale is not None else None
+
+    class _P:
+        def __init__(self, arr):
+            self.arr = arr
+
+        def data_ptr(self):
+            return self.arr.ctypes.data
+
+    wrap = {k: (_P(v) if v is not None else None) for k, v in bufs.items()}
+
+    class _W(dict):
+        def __getitem__(self, k):
+            return dict.__getitem__(self, k)
+
+    wb = _W(wrap)
+    wb["work"] = _P(bufs["work"])
+    # make_args zeroes the work counter through .zero_(); emulate that
+    bufs["work"][:] = 0
+    wb["work"].zero_ = lambda: None
+    args = solver.make_args(prep, wb, _P(inits), _P(params), None, n_runs, duration, settling_time, t0,
+                            _P(dur) if dur is not None else None, _P(tsc) if tsc is not None else None)
+    block = 32
+    grid = (n_runs + block - 1) // block
+    lib.emu_launch(ctypes.byref(args), 0 if kernel == "plain" else 1, grid, block)
+    bufs["n_save"] = n_save
+    bufs["n_summ"] = n_summ
+    return bufs
