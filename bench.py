@@ -1,0 +1,413 @@
+#!/usr/bin/env python
+"""Benchmark: solved systems/s on 2^20 stiff Van der Pol initial value problems.
+
+Workload (one step): 2^20 runs of x' = y, y' = mu (1 - x^2) y - x with
+mu = 10^U[0,3], (x0, y0) ~ U[-2,2]^2 and per-run horizon t in [0, 2 mu],
+rtol = atol = 1e-6, final state saved; seed 2.  The engine path integrates
+it with ROS3P (unpreconditioned GMRES stage solves), FP32 stepping with FP64
+time, control and norms, in the persistent work-stealing launch.
+
+A run counts as solved when its status word is 0 and its final state lies
+within 10 tolerance units (|y - y*| <= 10 (atol + rtol |y*|)) of an FP64
+reference solution y* (Radau IIA5, rtol = atol = 1e-10) computed untimed on
+a seeded subset of the runs; ``value`` = runs x solved fraction / seconds.
+
+Also measured and reported: the same workload through the public API with
+host buffers (``e2e``), Radau IIA5 on the same path, the plain
+one-thread-per-run FP32 kernel with the reference's default ROS3P settings
+(minimal-residual Krylov + Neumann preconditioner) on a subset, the
+roofline of the integration kernel, and a CPU baseline.
+
+``--impl reference`` times the reference algorithm's CPU restatement
+(the oracle: ROS3P with the reference defaults) on a bounded sample with all
+host cores.  Launch: ``python bench.py [--gpus N --steps K --warmup W]``;
+under torchrun each rank integrates its own 2^20-run shard (weak scaling).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+VDP = ["dx = y", "dy = mu * (1 - x**2) * y - x"]
+RTOL = ATOL = 1e-6
+SOLVED_TOL_UNITS = 10.0
+SEED = 2
+NEW = dict(algorithm="ros3p", rtol=RTOL, atol=ATOL, linear_correction_type="gmres", preconditioner_type=None,
+           mixed_precision=True, kernel="persistent")
+NEW_RADAU = dict(NEW, algorithm="radau")
+PLAIN = dict(algorithm="ros3p", rtol=RTOL, atol=ATOL, kernel="plain", max_steps=1_000_000)
+TRUTH = dict(algorithm="radau", rtol=1e-10, atol=1e-10, dt_min=1e-12, linear_correction_type="gmres",
+             preconditioner_type=None, kernel="persistent")
+WORKLOAD = ("stiff Van der Pol, 2 states, mu=10^U[0,3], x0~U[-2,2]^2, t in [0, 2 mu] per run, "
+            "rtol=atol=1e-6, final state only")
+
+
+def workload(n: int, seed: int):
+    rng = np.random.default_rng(seed)
+    mu = 10.0 ** rng.uniform(0.0, 3.0, n)
+    x0 = rng.uniform(-2.0, 2.0, (2, n))
+    return x0, mu, 2.0 * mu
+
+
+def log(*a):
+    print("[bench]", *a, file=sys.stderr, flush=True)
+
+
+def tol_units(y, truth):
+    return np.max(np.abs(np.asarray(y, np.float64) - truth) / (ATOL + RTOL * np.abs(truth)), axis=0)
+
+
+# ---------------------------------------------------------------------------
+# CPU side (oracle restatement of the reference algorithm; SciPy FP64 truth)
+# ---------------------------------------------------------------------------
+def _scipy_truth(args):
+    x0, mu = args
+    from scipy.integrate import solve_ivp
+    out = []
+    for i in range(len(mu)):
+        m = float(mu[i])
+        s = solve_ivp(lambda t, y: [y[1], m * (1 - y[0] ** 2) * y[1] - y[0]], (0.0, 2.0 * m), x0[:, i],
+                      method="Radau", rtol=1e-10, atol=1e-10,
+                      jac=lambda t, y: [[0.0, 1.0], [-2.0 * m * y[0] * y[1] - 1.0, m * (1.0 - y[0] ** 2)]])
+        out.append(s.y[:, -1])
+    return np.array(out).T
+
+
+def _oracle_chunk(args):
+    x0, mu, max_steps = args
+    from oracle import OracleSystem, integrate
+    osys = OracleSystem(VDP, ["x", "y"], ["mu"], {})
+    t = time.perf_counter()
+    out = integrate(osys, "ros3p", x0, mu[None, :], float((2 * mu).max()), durations=2 * mu,
+                    precision=np.float32, rtol=RTOL, atol=ATOL, max_steps=max_steps)
+    return out["state"][-1], out["status"], time.perf_counter() - t
+
+
+def cpu_reference(per_core: int = 2, max_steps: int = 3000, seed: int = SEED):
+    """Reference algorithm (ROS3P, reference defaults, FP32) on the host cores."""
+    import multiprocessing as mp
+    cores = os.cpu_count() or 1
+    n = per_core * cores
+    x0, mu, _ = workload(n, seed)
+    chunks = [(x0[:, i::cores], mu[i::cores]) for i in range(cores)]
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(cores) as pool:
+        truths = pool.map(_scipy_truth, chunks)
+        t0 = time.perf_counter()
+        res = pool.map(_oracle_chunk, [(c[0], c[1], max_steps) for c in chunks])
+        wall = time.perf_counter() - t0
+    solved = 0
+    for (y, st, _), tr in zip(res, truths):
+        err = tol_units(y, tr)
+        solved += int(np.sum((st == 0) & (err <= SOLVED_TOL_UNITS)))
+    return dict(value=solved / wall, unit="systems/s", cores=cores, kind="port", solved=solved, sample_n=n,
+                wall_s=wall,
+                sample=(f"{n} runs of the workload (seed {seed}), reference-default ROS3P (FP32, minimal residual "
+                        f"+ Neumann order 2, Gustafsson), oracle restatement, {cores} processes, "
+                        f"{max_steps}-step budget per run (unfinished runs count as unsolved); truth: SciPy "
+                        f"Radau rtol=atol=1e-10"))
+
+
+# ---------------------------------------------------------------------------
+# GPU side
+# ---------------------------------------------------------------------------
+class Clocks:
+    def __init__(self, path: Path, device: int):
+        self.path = path
+        self.proc = None
+        self.device = device
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.fh.close()
+
+    def summary(self):
+        if self.proc is None or not self.path.exists():
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        rows = []
+        for line in self.path.read_text().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return json.loads(p.read_text())
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "fallback": True}
+
+
+def gpu_arm(args, rank: int, world: int, dist):
+    import torch
+    from cubie_b200 import Solver, create_ODE_system, _native
+    from cubie_b200.perfmodel import estimate_flops
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    n = args.n
+    x0, mu, durs = workload(n, SEED + 1000 * rank)
+    sys32 = create_ODE_system(VDP, states={"x": 2.0, "y": 0.0}, parameters={"mu": 10.0}, precision=np.float32)
+    sys64 = create_ODE_system(VDP, states={"x": 2.0, "y": 0.0}, parameters={"mu": 10.0}, precision=np.float64)
+    T = min(args.truth_n, n)
+
+    # FP64 truth on a seeded subset (the runs are i.i.d., so the first T are a random sample)
+    truth_solver = Solver(sys64, output_types=["state"], max_steps=5_000_000, device=dev.index, **TRUTH)
+    tr = truth_solver.solve(x0[:, :T], mu[None, :T], duration=float(durs[:T].max()), durations=durs[:T],
+                            nan_error_trajectories=False)
+    truth = tr.state[-1].astype(np.float64)
+    log('truth', T, 'runs', truth_solver.last_kernel_ms, 'ms', tr.totals, 'bad', int((tr.status_codes != 0).sum()))
+    truth_ok = tr.status_codes == 0
+
+    def solved_fraction(y_subset, status_subset):
+        err = tol_units(y_subset, truth)
+        ok = (status_subset == 0) & (err <= SOLVED_TOL_UNITS) & truth_ok
+        return float(ok.sum()) / float(truth_ok.sum()), err
+
+    def device_timing(cfg, sysm, steps, warmup, n_runs):
+        solver = Solver(sysm, output_types=["state"], device=dev.index, **cfg)
+        prep = solver.prepare(float(durs[:n_runs].max()), durations=durs[:n_runs])
+        tdt = torch.float32 if sysm.precision == np.float32 else torch.float64
+        inits_t = torch.as_tensor(x0[:, :n_runs], device=dev).to(tdt).contiguous()
+        params_t = torch.as_tensor(mu[None, :n_runs], device=dev).to(tdt).contiguous()
+        dur_t = torch.as_tensor(durs[:n_runs], device=dev, dtype=torch.float64)
+        bufs = solver.allocate_outputs(prep, n_runs, dev, tdt)
+        flush = torch.empty(int(256e6) // 4, dtype=torch.int32, device=dev)
+        kernel = 1 if cfg["kernel"] == "persistent" else 0
+        stream = torch.cuda.current_stream(dev)
+        times = []
+        totals = None
+        for it in range(warmup + steps):
+            bufs["totals"].zero_()
+            args_ = solver.make_args(prep, bufs, inits_t, params_t, None, n_runs, float(durs[:n_runs].max()),
+                                     0.0, 0.0, dur_t, None)
+            _native.flush_l2(flush.data_ptr(), flush.numel() * 4, stream.cuda_stream)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            prep["module"].launch(args_, kernel, solver.block_size, 0, stream.cuda_stream)
+            e1.record(stream)
+            e1.synchronize()
+            if it >= warmup:
+                times.append(e0.elapsed_time(e1))
+            tot = bufs["totals"].cpu().numpy()
+            totals = dict(steps=int(tot[0]), rejections=int(tot[1]), newton=int(tot[2]), krylov=int(tot[3]))
+        y = bufs["state"][-1].cpu().numpy()
+        st = bufs["status"].cpu().numpy()
+        info = prep["module"].kernel_info(kernel)
+        del flush
+        return dict(times=times, y=y, status=st, totals=totals, spec=prep["spec"], gen=prep["gen"].system,
+                    kernel_info=info, block=solver.block_size, n=n_runs)
+
+    # ---- warm the compile caches outside any timing
+    device_timing(NEW, sys32, 0, 1, min(n, 4096))
+
+    clocks = Clocks(ROOT / "gpurun_out" / f"clocks_rank{rank}.csv" if (ROOT / "gpurun_out").exists()
+                    else Path("/tmp") / f"cbx_clocks_rank{rank}.csv", dev.index)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with clocks:
+        new = device_timing(NEW, sys32, args.steps, args.warmup, n)
+    log('new', new['times'], new['totals'])
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    ms = float(np.mean(new["times"]))
+    frac, err = solved_fraction(new["y"][:, :T], new["status"][:T])
+    solved_est = n * frac
+    ms_max = ms
+    total_solved = solved_est
+    if dist is not None:
+        t = torch.tensor([ms, solved_est], device=dev, dtype=torch.float64)
+        tm = t.clone()
+        dist.all_reduce(tm[:1], op=dist.ReduceOp.MAX)
+        dist.all_reduce(t[1:], op=dist.ReduceOp.SUM)
+        ms_max, total_solved = float(tm[0]), float(t[1])
+    value = total_solved / (ms_max * 1e-3)
+
+    # ---- end to end through the public API with pinned host buffers
+    solver_e2e = Solver(sys32, output_types=["state"], device=dev.index, **NEW)
+    x0_h = torch.as_tensor(x0.astype(np.float32)).pin_memory()
+    mu_h = torch.as_tensor(mu[None, :].astype(np.float32)).pin_memory()
+    du_h = torch.as_tensor(durs).pin_memory()
+    res = solver_e2e.solve(x0_h, mu_h, duration=float(durs.max()), durations=du_h, nan_error_trajectories=False)
+    e2e_times = []
+    for _ in range(max(1, args.steps)):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        res = solver_e2e.solve(x0_h, mu_h, duration=float(durs.max()), durations=du_h, nan_error_trajectories=False)
+        torch.cuda.synchronize()
+        e2e_times.append(time.perf_counter() - t0)
+    log('e2e', e2e_times)
+    e2e_frac, _ = solved_fraction(res.state[-1][:, :T], res.status_codes[:T])
+    e2e_value = n * e2e_frac / float(np.mean(e2e_times))
+    h2d = x0_h.numel() * 4 + mu_h.numel() * 4 + du_h.numel() * 8
+    d2h = res.state.size * 4 + res.status_codes.size * 4 + 4 * 8
+
+    out = None
+    if rank == 0:
+        # ---- Radau IIA5 on the same path, plain baseline on a subset
+        radau = device_timing(NEW_RADAU, sys32, max(1, min(args.steps, 3)), 1, n)
+        r_ms = float(np.mean(radau["times"]))
+        log('radau', radau['times'], radau['totals'])
+        r_frac, r_err = solved_fraction(radau["y"][:, :T], radau["status"][:T])
+        P = min(args.plain_n, n)
+        plain = device_timing(PLAIN, sys32, 1, 0, P)
+        p_ms = float(np.mean(plain["times"]))
+        log('plain', plain['times'], plain['totals'])
+        PT = min(P, T)
+        p_err = tol_units(plain["y"][:, :PT], truth[:, :PT])
+        p_ok = (plain["status"][:PT] == 0) & (p_err <= SOLVED_TOL_UNITS) & truth_ok[:PT]
+        p_frac = float(p_ok.sum()) / float(truth_ok[:PT].sum())
+        plain_value = P * p_frac / (p_ms * 1e-3)
+
+        # ---- roofline: FP32 issue bound (measured FMA throughput)
+        flops = estimate_flops(new["spec"], new["gen"], new["totals"])
+        achieved = flops / (ms * 1e-3) / 1e12
+        peak_fp32 = _native.fp32_peak(dev.index) / 1e12
+        hbm_bytes = (x0.size * 4 + mu.size * 4 + durs.size * 8 + 2 * 2 * n * 4 + n * 4)
+        peaks = measured_peaks()
+        cpu = cpu_reference(per_core=args.cpu_per_core, max_steps=args.cpu_max_steps) if not args.no_cpu else None
+        out = {
+            "metric": "solved systems/s at matched FP64-oracle error (fwd), persistent mixed-precision path",
+            "value": value,
+            "unit": "systems/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": ms_max,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32 stepping, f64 time/control/norms",
+            "data": "synthetic (seeded)",
+            "config": {"workload": WORKLOAD, "n_systems_per_gpu": n, "algorithm": "ros3p",
+                       "linear_solver": "gmres (unpreconditioned)", "kernel": "persistent work-stealing",
+                       "precision": "mixed", "solved_if": f"status==0 and error<={SOLVED_TOL_UNITS} tol units",
+                       "truth": f"FP64 Radau IIA5 rtol=atol=1e-10 on {T} seeded runs",
+                       "l2": "flushed (256 MB write) before every timed launch",
+                       "block": new["block"]},
+            "solved_fraction": frac,
+            "error_tol_units_pct50_90_99": [float(np.percentile(err, q)) for q in (50, 90, 99)],
+            "totals_per_step": new["totals"],
+            "e2e": {"value": e2e_value, "unit": "systems/s", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h), "ms_per_step": 1e3 * float(np.mean(e2e_times))},
+            "gpu_launches": args.steps,
+            "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak_fp32, "unit": "TFLOP/s",
+                         "frac": achieved / peak_fp32, "traffic": None,
+                         "peak_source": "measured FP32 FMA probe (cbx_fp32_peak_probe) in this run",
+                         "flops_per_launch": flops,
+                         "hbm": {"algorithmic_bytes": hbm_bytes, "achieved_gbs": hbm_bytes / (ms * 1e-3) / 1e9,
+                                 "peak_gbs": peaks.get("hbm_gbs"),
+                                 "note": "HBM is not the bound: per-run I/O is 32 bytes"}},
+            "kernel_info": new["kernel_info"],
+            "radau": {"value": n * r_frac / (r_ms * 1e-3), "ms_per_step": r_ms, "solved_fraction": r_frac,
+                      "totals_per_step": radau["totals"]},
+            "plain": {"value": plain_value, "n_systems": P, "ms": p_ms, "solved_fraction": p_frac,
+                      "totals": plain["totals"],
+                      "config": "one thread per run, FP32, ROS3P with reference defaults "
+                                "(minimal residual + Neumann order 2)"},
+            "speedup_vs_plain": value / plain_value if plain_value > 0 else None,
+            "cpu_baseline": cpu,
+            "clocks": clocks.summary(),
+        }
+    return out
+
+
+def reference_arm(args):
+    cpu = cpu_reference(per_core=args.cpu_per_core, max_steps=args.cpu_max_steps)
+    vals = []
+    for _ in range(max(1, args.steps)):
+        vals.append(cpu_reference(per_core=args.cpu_per_core, max_steps=args.cpu_max_steps)["value"])
+    v = float(np.mean(vals))
+    cpu["value"] = v
+    return {
+        "impl": "reference",
+        "metric": "solved systems/s at matched FP64-oracle error (fwd), persistent mixed-precision path",
+        "value": v, "unit": "systems/s", "n_gpus": int(os.environ.get("WORLD_SIZE", "1")),
+        "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+        "config": {"workload": WORKLOAD, "algorithm": "ros3p (reference defaults)", "sample": cpu["sample"]},
+        "cpu_baseline": {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")},
+        "e2e": {"value": v, "unit": "systems/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="cubie_b200")
+    ap.add_argument("--n", type=int, default=1 << 20)
+    ap.add_argument("--truth-n", type=int, default=8192)
+    ap.add_argument("--plain-n", type=int, default=16384)
+    ap.add_argument("--cpu-per-core", type=int, default=2)
+    ap.add_argument("--cpu-max-steps", type=int, default=3000)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(reference_arm(args)), flush=True)
+        return
+    dist = None
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as tdist
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        dist = tdist
+    try:
+        out = gpu_arm(args, rank, world, dist)
+    finally:
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
+    if rank == 0 and out is not None:
+        print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()

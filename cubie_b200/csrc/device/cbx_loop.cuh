@@ -343,21 +343,31 @@ template <class Cfg>
 __device__ __forceinline__ void lane_end(const Lane<Cfg>& L, const cbx_solve_args a, BlockTotals* bt) {
     a.status_out[L.run] = L.status;
     if (a.totals) {
-        atomicAdd(&bt->v[0], (unsigned long long)L.steps);
-        atomicAdd(&bt->v[1], (unsigned long long)L.rejections);
-        atomicAdd(&bt->v[2], (unsigned long long)L.newton);
-        atomicAdd(&bt->v[3], (unsigned long long)L.krylov);
+#ifdef CBX_HOST_EMULATION
+        // one emulated thread at a time: no block-level staging
+        unsigned long long* dst = a.totals;
+#else
+        unsigned long long* dst = bt->v;
+#endif
+        atomicAdd(dst + 0, (unsigned long long)L.steps);
+        atomicAdd(dst + 1, (unsigned long long)L.rejections);
+        atomicAdd(dst + 2, (unsigned long long)L.newton);
+        atomicAdd(dst + 3, (unsigned long long)L.krylov);
     }
 }
 
 __device__ __forceinline__ void totals_begin(BlockTotals* bt) {
+#ifndef CBX_HOST_EMULATION
     if (threadIdx.x < 4) bt->v[threadIdx.x] = 0ull;
     __syncthreads();
+#endif
 }
 
 __device__ __forceinline__ void totals_flush(BlockTotals* bt, const cbx_solve_args a) {
+#ifndef CBX_HOST_EMULATION
     __syncthreads();
     if (a.totals && threadIdx.x < 4 && bt->v[threadIdx.x]) atomicAdd(a.totals + threadIdx.x, bt->v[threadIdx.x]);
+#endif
 }
 
 // Plain kernel: one thread integrates one run to completion

@@ -67,6 +67,10 @@ def _torch():
     return torch
 
 
+def _is_tensor(value) -> bool:
+    return type(value).__module__.startswith("torch") and hasattr(value, "data_ptr")
+
+
 def _as_tol(value, n) -> np.ndarray:
     arr = np.asarray(value, dtype=np.float64).reshape(-1)
     if arr.size == 1:
@@ -227,6 +231,13 @@ class Solver:
                 self.krylov_residual_reduction = floor
             else:
                 self.krylov_residual_reduction = eps
+            if self.mixed_precision:
+                # FP32 Krylov vectors cannot represent a residual reduction
+                # finer than a few float32 ulps; the derived default (0.01 rtol
+                # for Rosenbrock steps) would otherwise leave every solve at
+                # its iteration cap.
+                self.krylov_residual_reduction = max(self.krylov_residual_reduction,
+                                                     8.0 * float(np.finfo(np.float32).eps))
         self.krylov_residual_floor = float(user.get("krylov_residual_floor") or math.sqrt(eps))
         self.krylov_max_iters = int(user.get("krylov_max_iters", 100))
         self.newton_max_iters = int(user.get("newton_max_iters", 100))
@@ -433,7 +444,12 @@ class Solver:
             interp = ArrayInterpolator.from_system(self.system, drivers, self.precision)
         else:
             interp = None
-        inits, params = self.build_grid(initial_values, parameters, grid_type)
+        if _is_tensor(initial_values) and _is_tensor(parameters):
+            # pre-built [n_states, n_runs] / [n_params, n_runs] tensors (host,
+            # possibly pinned, or device): no grid building, no host copies
+            inits, params = initial_values, parameters
+        else:
+            inits, params = self.build_grid(initial_values, parameters, grid_type)
         return self.run(inits, params, interp, duration, settling_time, t0,
                         nan_error_trajectories=nan_error_trajectories, on_device=on_device,
                         durations=durations, tol_scale=tol_scale, stream=stream,
@@ -478,21 +494,24 @@ class Solver:
         n_runs = int(inits.shape[1])
         inits_t = inits if isinstance(inits, torch.Tensor) else torch.as_tensor(np.ascontiguousarray(inits), device=dev)
         params_t = params if isinstance(params, torch.Tensor) else torch.as_tensor(np.ascontiguousarray(params), device=dev)
-        inits_t = inits_t.to(device=dev, dtype=tdtype).contiguous()
-        params_t = params_t.to(device=dev, dtype=tdtype).contiguous()
+        inits_t = inits_t.to(device=dev, dtype=tdtype, non_blocking=True).contiguous()
+        params_t = params_t.to(device=dev, dtype=tdtype, non_blocking=True).contiguous()
         if params_t.numel() == 0:
             params_t = torch.zeros((1, max(n_runs, 1)), device=dev, dtype=tdtype)
         bufs = self.allocate_outputs(prep, n_runs, dev, tdtype)
-        dur_t = None
-        if durations is not None:
-            dur_t = torch.as_tensor(np.asarray(durations, dtype=np.float64).reshape(-1), device=dev)
-            if dur_t.numel() != n_runs:
-                raise ValueError("durations must have one entry per run")
-        tol_t = None
-        if tol_scale is not None:
-            tol_t = torch.as_tensor(np.asarray(tol_scale, dtype=np.float64).reshape(-1), device=dev)
-            if tol_t.numel() != n_runs:
-                raise ValueError("tol_scale must have one entry per run")
+        def per_run(values, name):
+            if values is None:
+                return None
+            if _is_tensor(values):
+                t = values.to(device=dev, dtype=torch.float64, non_blocking=True).reshape(-1).contiguous()
+            else:
+                t = torch.as_tensor(np.asarray(values, dtype=np.float64).reshape(-1), device=dev)
+            if t.numel() != n_runs:
+                raise ValueError(f"{name} must have one entry per run")
+            return t
+
+        dur_t = per_run(durations, "durations")
+        tol_t = per_run(tol_scale, "tol_scale")
         coeff_t = None
         if interp is not None:
             coeff_t = torch.as_tensor(interp.coefficients.astype(self.precision), device=dev).contiguous()

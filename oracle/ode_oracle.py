@@ -408,12 +408,14 @@ class Settings:
     krylov_max_iters: int = 100
     newton_max_iters: int = 100
     preconditioner_order: int = 2
+    preconditioner_type: Optional[str] = "neumann"
     krylov_residual_reduction: Optional[float] = None
     save_every: Optional[float] = None
     summarise_every: Optional[float] = None
     sample_summaries_every: Optional[float] = None
     output_types: Sequence[str] = ("state",)
     dense_prediction: bool = True
+    max_steps: int = 0
 
 
 def integrate(system: OracleSystem, algorithm: str, inits: np.ndarray, params: np.ndarray,
@@ -484,10 +486,14 @@ def integrate(system: OracleSystem, algorithm: str, inits: np.ndarray, params: n
     def lin_solve(A, Pc, norm2, rhs, x):
         if S.linear_correction_type == "bicgstab":
             return bicgstab_solve(A, Pc, norm2, rhs, x, floor_c, red_c, S.krylov_max_iters, rt, ct)
-        if S.linear_correction_type == "gmres":
-            # GMRES has no reference counterpart; the oracle solves the
-            # small dense system directly (the converged answer GMRES targets).
-            raise NotImplementedError("gmres is checked against direct solves in the tests")
+        if S.linear_correction_type in ("gmres", "direct"):
+            # GMRES has no reference counterpart; the oracle solves the small
+            # dense system directly, which is the answer GMRES converges to.
+            K = rhs.shape[1]
+            eye = np.eye(K, dtype=rhs.dtype)
+            M = np.stack([A(np.broadcast_to(eye[k], rhs.shape).copy()) for k in range(K)], axis=2)
+            sol = np.linalg.solve(M.astype(np.float64), rhs.astype(np.float64)[:, :, None])[:, :, 0]
+            return sol.astype(rhs.dtype), np.zeros(rhs.shape[0], np.int64), np.ones(rhs.shape[0], np.int64)
         return mr_solve(A, Pc, norm2, rhs, x, floor_c, red_c, S.krylov_max_iters,
                         S.linear_correction_type == "steepest_descent", rt, ct)
 
@@ -643,6 +649,7 @@ def integrate(system: OracleSystem, algorithm: str, inits: np.ndarray, params: n
     summ_idx = np.zeros(B, np.int64)
     upd_idx = np.zeros(B, np.int64)
     counters = np.zeros((B, 4), np.int64)
+    counters_total = np.zeros(B, np.int64)
     allm = np.ones(B, bool)
     if settling_time == 0.0:
         if save_every is not None:
@@ -763,7 +770,7 @@ def integrate(system: OracleSystem, algorithm: str, inits: np.ndarray, params: n
             for _ in range(S.preconditioner_order):
                 out = v + s_coef[:, None] * np.einsum("bij,bj->bi", J, out)
             return out
-        return A, Pc, (lambda v: scaled_norm2(v, ref, kry_tol, ct))
+        return A, (Pc if S.preconditioner_type == "neumann" else None), (lambda v: scaled_norm2(v, ref, kry_tol, ct))
 
     iteration = 0
     while True:
@@ -790,6 +797,11 @@ def integrate(system: OracleSystem, algorithm: str, inits: np.ndarray, params: n
             at_end = (tp < t_end) & finished
             finished = finished & ~at_end
         finished = finished | irrec
+        if S.max_steps:
+            # step budget (status bit 32), as the engine's ``max_steps``
+            over = active & ~finished & (counters_total >= S.max_steps)
+            status = np.where(over, status | 32, status)
+            finished = finished | over
         done = done | (finished & active)
         act = ~done
         if not act.any():
@@ -942,7 +954,8 @@ def integrate(system: OracleSystem, algorithm: str, inits: np.ndarray, params: n
                     for _ in range(S.preconditioner_order):
                         out = v + h[:, None] * cjv(out)
                     return out
-                return A, Pc, (lambda v: scaled_norm2(v, Y, kry_tol, ct))
+                return A, (Pc if S.preconditioner_type == "neumann" else None), \
+                    (lambda v: scaled_norm2(v, Y, kry_tol, ct))
 
             def corr(delta_, u):
                 tot = np.zeros(B, ct)
@@ -1130,6 +1143,7 @@ def integrate(system: OracleSystem, algorithm: str, inits: np.ndarray, params: n
         counters[:, 0] += np.where(act, nit, 0)
         counters[:, 1] += np.where(act, kitv, 0)
         counters[:, 2] += act
+        counters_total += act
         counters[:, 3] += act & ~accept
         t_prop = t + dt_eff.astype(np.float64)
         stagn = np.where(act, np.where(t_prop == t, stagn + 1, 0), stagn)

@@ -5,6 +5,7 @@
 // device logic can be checked against the oracle without a GPU.  Warp
 // intrinsics act on a single lane (each emulated thread runs alone).
 #pragma once
+#define CBX_HOST_EMULATION 1
 #include <cmath>
 #include <cstddef>
 #include <cstdint>

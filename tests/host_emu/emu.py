@@ -40,7 +40,10 @@ _cache = {}
 
 
 def compile_emulated(source: str):
-    key = hashlib.sha256((source + (HERE / "cbx_host_emu.h").read_text()).encode()).hexdigest()[:20]
+    h = hashlib.sha256((source + (HERE / "cbx_host_emu.h").read_text()).encode())
+    for f in sorted(Path(DEVICE).glob("*")):
+        h.update(f.read_bytes())
+    key = h.hexdigest()[:20]
     if key in _cache:
         return _cache[key]
     d = Path(tempfile.gettempdir()) / "cbx_emu"
