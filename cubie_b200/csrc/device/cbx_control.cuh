@@ -10,7 +10,13 @@
 // truncated onto an output event keeps dt (freeze) and leaves the history
 // untouched.  STEP_TOO_SMALL is returned when dt * gain <= dt_min.
 // Everything is computed in the control precision C (FP64 on the
-// mixed-precision path).
+// mixed-precision path) except the exponentiations of the gain there,
+// which run in FP32: the gain is clamped to [min_gain, max_gain] before it
+// scales the FP64 step size, so its 24-bit value gives the same step
+// sequence to within that rounding, and an FP64 pow costs far more issue
+// slots than the rest of the step update.  Out-of-range arguments behave
+// alike in both widths after the clamp (an FP32 overflow to inf gives a
+// zero or infinite factor where FP64 gives a tiny or huge one).
 #pragma once
 #include "cbx_common.cuh"
 
@@ -27,6 +33,10 @@ struct Controller {
     static __device__ __forceinline__ void init(State& st) {
         st.h0 = C(0);
         st.h1 = C(0);
+    }
+    static __device__ __forceinline__ C cpow(C a, C b) {
+        if constexpr (Cfg::MIXED) return C(pow_t(float(a), float(b)));
+        else return pow_t(a, b);
     }
     static __device__ __forceinline__ C error_norm2(const R* ynew, const R* y, const R* err, C tol_scale) {
         C nrm2 = C(0);
@@ -63,20 +73,20 @@ struct Controller {
             bool commit_history = accept && !truncated;
             const C current_dt = dt;
             if constexpr (Cfg::CTRL == CTRL_I) {
-                gain = C(safety * pow_t(nrm2, -C(Cfg::CTL_E1)));
+                gain = C(safety * cpow(nrm2, -C(Cfg::CTL_E1)));
             } else if constexpr (Cfg::CTRL == CTRL_PI) {
                 const C err_prev = st.h0;
-                const C pgain = pow_t(nrm2, -C(Cfg::CTL_E1));
+                const C pgain = cpow(nrm2, -C(Cfg::CTL_E1));
                 const C src = err_prev > C(0) ? err_prev : nrm2;
-                const C igain = pow_t(src, -C(Cfg::CTL_E2));
+                const C igain = cpow(src, -C(Cfg::CTL_E2));
                 gain = safety * pgain * igain;
                 st.h0 = commit_history ? nrm2 : err_prev;
             } else if constexpr (Cfg::CTRL == CTRL_PID) {
                 const C err_prev = st.h0, err_prev_prev = st.h1;
                 const C eps = err_prev > C(0) ? err_prev : nrm2;
                 const C epps = err_prev_prev > C(0) ? err_prev_prev : eps;
-                gain = C(safety * pow_t(nrm2, -C(Cfg::CTL_E1)) * pow_t(eps, -C(Cfg::CTL_E2)) *
-                         pow_t(epps, -C(Cfg::CTL_E3)));
+                gain = C(safety * cpow(nrm2, -C(Cfg::CTL_E1)) * cpow(eps, -C(Cfg::CTL_E2)) *
+                         cpow(epps, -C(Cfg::CTL_E3)));
                 st.h1 = commit_history ? err_prev : err_prev_prev;
                 st.h0 = commit_history ? nrm2 : err_prev;
             } else {  // Gustafsson (gustafsson_controller.py:236-283)
@@ -87,9 +97,9 @@ struct Controller {
                 const C denom = C(niters + 2 * Cfg::CTL_NEWTON_TARGET);
                 const C tmp = gain_numerator / denom;
                 const C fac = safety < tmp ? safety : tmp;
-                const C gain_basic = C(fac * pow_t(nrm2, -expo));
+                const C gain_basic = C(fac * cpow(nrm2, -expo));
                 const C ratio = nrm2 * nrm2 / err_prev;
-                const C gain_gus = C(safety * (dt / dt_prev) * pow_t(ratio, -expo));
+                const C gain_gus = C(safety * (dt / dt_prev) * cpow(ratio, -expo));
                 gain = gain_gus < gain_basic ? gain_gus : gain_basic;
                 gain = (accept && dt_prev > C(1e-16)) ? gain : gain_basic;
                 st.h0 = commit_history ? current_dt : st.h0;

@@ -203,41 +203,59 @@ __device__ __forceinline__ int solve_bicgstab(const Op& op, typename Cfg::R* rhs
 // The system is scaled by W = diag(1 / (tol_i sqrt(K))), so the 2-norm of
 // the scaled residual equals the reference's weighted RMS norm and the
 // Givens-rotated residual estimate |g_{j+1}| is checked directly against
-// floor + reduction * ||b||.  Basis vectors are stored in R, inner
-// products, the Hessenberg matrix and rotations in C (FP64 in mixed
-// precision).  One Arnoldi step (one operator and one preconditioner
-// application) counts as one iteration.
+// floor + reduction * ||b||.  The weights are formed once per solve; the
+// basis, inner products, Hessenberg matrix and rotations are kept in the
+// working precision R (FP32 on the mixed-precision path, where the
+// reduction is floored at 8 FP32 epsilons, so wider scalars would not
+// change the answer and only cost FP64 and conversion issue slots).  One
+// Arnoldi step (one operator and one preconditioner application) counts
+// as one iteration.
 template <class Cfg, class Op>
 __device__ __forceinline__ int solve_gmres(const Op& op, typename Cfg::R* rhs,
                                            typename Cfg::R* x, int& iters) {
     using R = typename Cfg::R;
-    using C = typename Cfg::C;
     constexpr int K = Op::K;
     constexpr int M = (Cfg::GMRES_RESTART < K) ? Cfg::GMRES_RESTART : K;
     R V[M + 1][K];
-    C H[M][M];
-    C g[M + 1], cs[M], sn[M], yv[M];
+    R H[M][M];
+    R g[M + 1], cs[M], sn[M], yv[M];
     R b[K], w[K], z[K];
-    const C sK = sqrt_t(C(K));
+    R wt[K], iwt[K];  // W and W^-1
+    {
+        const R sK = sqrt_t(R(K));
+#pragma unroll
+        for (int i = 0; i < K; ++i) {
+            iwt[i] = R(op.tol(i)) * sK;
+            wt[i] = R(1) / iwt[i];
+        }
+    }
+    auto scaled_norm = [&](const R* v) {
+        R s = R(0);
+#pragma unroll
+        for (int i = 0; i < K; ++i) {
+            const R u = v[i] * wt[i];
+            s += u * u;
+        }
+        return sqrt_t(s);
+    };
 
-    const C rhs_norm2 = op.wnorm2(rhs);
-    const C tol = C(Cfg::KRYLOV_FLOOR) + C(Cfg::KRYLOV_REDUCTION) * sqrt_t(rhs_norm2);
+    const R tol = R(Cfg::KRYLOV_FLOOR) + R(Cfg::KRYLOV_REDUCTION) * scaled_norm(rhs);
     op.apply(x, w);
 #pragma unroll
     for (int i = 0; i < K; ++i) {
         b[i] = rhs[i];
         rhs[i] = rhs[i] - w[i];
     }
-    C beta = sqrt_t(op.wnorm2(rhs));
+    R beta = scaled_norm(rhs);
     bool converged = beta <= tol;
     int it = 0;
     while (!converged && it < Cfg::KRYLOV_MAX_ITERS) {
-        const C inv_beta = C(1) / beta;
+        const R inv_beta = R(1) / beta;
 #pragma unroll
-        for (int i = 0; i < K; ++i) V[0][i] = R(C(rhs[i]) / (op.tol(i) * sK) * inv_beta);
+        for (int i = 0; i < K; ++i) V[0][i] = rhs[i] * wt[i] * inv_beta;
         g[0] = beta;
 #pragma unroll
-        for (int j = 1; j <= M; ++j) g[j] = C(0);
+        for (int j = 1; j <= M; ++j) g[j] = R(0);
         int jend = 0;
         bool cycle_converged = false;
 #pragma unroll
@@ -246,7 +264,7 @@ __device__ __forceinline__ int solve_gmres(const Op& op, typename Cfg::R* rhs,
             ++it;
             // z = P^-1 W^-1 V_j ; w = W A z
 #pragma unroll
-            for (int i = 0; i < K; ++i) w[i] = R(C(V[j][i]) * op.tol(i) * sK);
+            for (int i = 0; i < K; ++i) w[i] = V[j][i] * iwt[i];
             if (Cfg::PRECONDITIONED) {
                 op.precond(w, z, V[M]);
             } else {
@@ -255,40 +273,41 @@ __device__ __forceinline__ int solve_gmres(const Op& op, typename Cfg::R* rhs,
             }
             op.apply(z, w);
 #pragma unroll
-            for (int i = 0; i < K; ++i) w[i] = R(C(w[i]) / (op.tol(i) * sK));
-            C hcol[M + 1];
+            for (int i = 0; i < K; ++i) w[i] = w[i] * wt[i];
+            R hcol[M + 1];
 #pragma unroll
             for (int l = 0; l < M; ++l) {
                 if (l <= j) {
-                    C dot = C(0);
+                    R dot = R(0);
 #pragma unroll
-                    for (int i = 0; i < K; ++i) dot += C(w[i]) * C(V[l][i]);
+                    for (int i = 0; i < K; ++i) dot += w[i] * V[l][i];
                     hcol[l] = dot;
 #pragma unroll
-                    for (int i = 0; i < K; ++i) w[i] = R(C(w[i]) - dot * C(V[l][i]));
+                    for (int i = 0; i < K; ++i) w[i] = w[i] - dot * V[l][i];
                 }
             }
-            C hn = C(0);
+            R hn = R(0);
 #pragma unroll
-            for (int i = 0; i < K; ++i) hn += C(w[i]) * C(w[i]);
+            for (int i = 0; i < K; ++i) hn += w[i] * w[i];
             hn = sqrt_t(hn);
             {
-                const C inv = (hn > C(0)) ? C(1) / hn : C(0);
+                const R inv = (hn > R(0)) ? R(1) / hn : R(0);
 #pragma unroll
-                for (int i = 0; i < K; ++i) V[j + 1][i] = R(C(w[i]) * inv);
+                for (int i = 0; i < K; ++i) V[j + 1][i] = w[i] * inv;
             }
 #pragma unroll
             for (int l = 0; l < M - 1; ++l) {
                 if (l < j) {
-                    const C a0 = hcol[l], a1 = hcol[l + 1];
+                    const R a0 = hcol[l], a1 = hcol[l + 1];
                     hcol[l] = cs[l] * a0 + sn[l] * a1;
                     hcol[l + 1] = -sn[l] * a0 + cs[l] * a1;
                 }
             }
-            const C a = hcol[j];
-            const C den = sqrt_t(a * a + hn * hn);
-            const C c = (den > C(0)) ? a / den : C(1);
-            const C s = (den > C(0)) ? hn / den : C(0);
+            const R a = hcol[j];
+            const R den = sqrt_t(a * a + hn * hn);
+            const R inv_den = (den > R(0)) ? R(1) / den : R(0);
+            const R c = (den > R(0)) ? a * inv_den : R(1);
+            const R s = hn * inv_den;
             cs[j] = c;
             sn[j] = s;
             hcol[j] = den;
@@ -298,7 +317,7 @@ __device__ __forceinline__ int solve_gmres(const Op& op, typename Cfg::R* rhs,
             for (int l = 0; l < M; ++l)
                 if (l <= j) H[l][j] = hcol[l];
             jend = j + 1;
-            if (absv(g[j + 1]) <= tol || hn == C(0)) {
+            if (absv(g[j + 1]) <= tol || hn == R(0)) {
                 cycle_converged = true;
                 break;
             }
@@ -308,21 +327,21 @@ __device__ __forceinline__ int solve_gmres(const Op& op, typename Cfg::R* rhs,
 #pragma unroll
         for (int l = M - 1; l >= 0; --l) {
             if (l < jend) {
-                C s = g[l];
+                R s = g[l];
 #pragma unroll
                 for (int m = 0; m < M; ++m)
                     if (m > l && m < jend) s -= H[l][m] * yv[m];
-                yv[l] = (H[l][l] != C(0)) ? s / H[l][l] : C(0);
+                yv[l] = (H[l][l] != R(0)) ? s / H[l][l] : R(0);
             }
         }
         // x += P^-1 W^-1 sum_l y_l V_l
 #pragma unroll
         for (int i = 0; i < K; ++i) {
-            C u = C(0);
+            R u = R(0);
 #pragma unroll
             for (int l = 0; l < M; ++l)
-                if (l < jend) u += yv[l] * C(V[l][i]);
-            w[i] = R(u * op.tol(i) * sK);
+                if (l < jend) u += yv[l] * V[l][i];
+            w[i] = u * iwt[i];
         }
         if (Cfg::PRECONDITIONED) {
             op.precond(w, z, V[M]);
@@ -344,7 +363,7 @@ __device__ __forceinline__ int solve_gmres(const Op& op, typename Cfg::R* rhs,
         op.apply(x, w);
 #pragma unroll
         for (int i = 0; i < K; ++i) rhs[i] = b[i] - w[i];
-        beta = sqrt_t(op.wnorm2(rhs));
+        beta = scaled_norm(rhs);
         converged = beta <= tol;
     }
     iters = it;

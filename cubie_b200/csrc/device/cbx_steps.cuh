@@ -219,56 +219,78 @@ struct RosenbrockStep {
             if (Tab::HAS_ERR) err[i] = R(0);
         }
         R K[S][N];
-        R f[N], rhs[N];
+        R f[N], rhs[N], Y[N];
+        R drv_stage[ND > 0 ? ND : 1];
         int status = SUCCESS;
         SingleStageOp<Cfg> op{J, gamma * dt, y, ctx.tol_scale};
-        Sys::template dxdt<R>(y, ctx.p, drv, t, f);
+        // One loop over the stages with a single call site of the linear
+        // solver keeps one copy of it in the instruction stream.  The stage
+        // index is a run-time value here, so tableau entries and the stored
+        // stage increments are picked with compile-time-unrolled selects
+        // (the increments stay in registers).  The initial guess of every
+        // stage is the solution of the one before it (the first stage uses
+        // the previous step's last increment), which is what ``ps.guess``
+        // already holds when the solve starts.
+#pragma unroll 1
+        for (int stage = 0; stage < S; ++stage) {
+            R c_s = R(0), gs_s = R(0), b_s = R(0), d_s = R(0);
 #pragma unroll
-        for (int i = 0; i < N; ++i) rhs[i] = ((f[i] + R(Tab::gs(0)) * tdv[i]) * dt) * gamma;
-        {
-            int it = 0;
-            status |= linear_solve<Cfg>(op, rhs, ps.guess, it);
-            its.kit_all += it;
-        }
-#pragma unroll
-        for (int i = 0; i < N; ++i) {
-            K[0][i] = ps.guess[i];
-            delta[i] += K[0][i] * R(Tab::b(0));
-            if (Tab::HAS_ERR) err[i] += K[0][i] * R(Tab::d(0));
-        }
-        R drv_stage[ND > 0 ? ND : 1];
-        R Y[N];
-#pragma unroll
-        for (int stage = 1; stage < S; ++stage) {
-            const R stage_time = t + dt * R(Tab::c(stage));
+            for (int q = 0; q < S; ++q) {
+                if (q == stage) {
+                    c_s = R(Tab::c(q));
+                    gs_s = R(Tab::gs(q));
+                    b_s = R(Tab::b(q));
+                    d_s = R(Tab::d(q));
+                }
+            }
+            const R stage_time = t + dt * c_s;
 #pragma unroll
             for (int i = 0; i < N; ++i) {
                 R v = y[i];
-#pragma unroll
-                for (int j = 0; j < S - 1; ++j)
-                    if (j < stage && Tab::a(stage, j) != 0.0) v += R(Tab::a(stage, j)) * K[j][i];
-                Y[i] = v;
-            }
-            if constexpr (ND > 0) Drivers<Cfg>::eval(stage_time, ctx.coeffs, drv_stage);
-            Sys::template dxdt<R>(Y, ctx.p, drv_stage, stage_time, f);
-#pragma unroll
-            for (int i = 0; i < N; ++i) {
                 R corr = R(0);
 #pragma unroll
-                for (int j = 0; j < S - 1; ++j)
-                    if (j < stage && Tab::Cm(stage, j) != 0.0) corr += R(Tab::Cm(stage, j)) * K[j][i];
-                const R rv = f[i] + corr * inv_dt + R(Tab::gs(stage)) * tdv[i];
+                for (int j = 0; j < S - 1; ++j) {
+                    R a_sj = R(0), c_sj = R(0);
+#pragma unroll
+                    for (int q = 1; q < S; ++q) {
+                        if (q == stage) {
+                            a_sj = R(Tab::a(q, j));
+                            c_sj = R(Tab::Cm(q, j));
+                        }
+                    }
+                    if (j < stage) {
+                        if (a_sj != R(0)) v += a_sj * K[j][i];
+                        if (c_sj != R(0)) corr += c_sj * K[j][i];
+                    }
+                }
+                Y[i] = v;
+                rhs[i] = corr;
+            }
+            if constexpr (ND > 0) {
+                if (stage == 0) {
+#pragma unroll
+                    for (int k = 0; k < ND; ++k) drv_stage[k] = drv[k];
+                } else {
+                    Drivers<Cfg>::eval(stage_time, ctx.coeffs, drv_stage);
+                }
+            }
+            Sys::template dxdt<R>(Y, ctx.p, ND > 0 ? drv_stage : drv, stage_time, f);
+#pragma unroll
+            for (int i = 0; i < N; ++i) {
+                const R rv = (stage > 0) ? f[i] + rhs[i] * inv_dt + gs_s * tdv[i] : f[i] + gs_s * tdv[i];
                 rhs[i] = rv * dt * gamma;
-                ps.guess[i] = K[stage - 1][i];
             }
             int it = 0;
             status |= linear_solve<Cfg>(op, rhs, ps.guess, it);
             its.kit_all += it;
 #pragma unroll
             for (int i = 0; i < N; ++i) {
-                K[stage][i] = ps.guess[i];
-                delta[i] += R(Tab::b(stage)) * K[stage][i];
-                if (Tab::HAS_ERR) err[i] += R(Tab::d(stage)) * K[stage][i];
+                const R k = ps.guess[i];
+#pragma unroll
+                for (int j = 0; j < S; ++j)
+                    if (j == stage) K[j][i] = k;
+                delta[i] += b_s * k;
+                if (Tab::HAS_ERR) err[i] += d_s * k;
             }
         }
 #pragma unroll
