@@ -63,6 +63,7 @@ EXPORTED = (
     "cbx_version", "cbx_last_error", "cbx_nvrtc_version", "cbx_compile", "cbx_free",
     "cbx_module_load", "cbx_module_create", "cbx_module_destroy", "cbx_kernel_info",
     "cbx_occupancy", "cbx_solve", "cbx_device_info", "cbx_fp32_peak_probe", "cbx_flush_l2",
+    "cbx_solve_noalloc",
 )
 
 _lib = None
@@ -115,6 +116,8 @@ def lib():
         L.cbx_fp32_peak_probe.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_double),
                                           ctypes.POINTER(ctypes.c_float)]
         L.cbx_flush_l2.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]
+        L.cbx_solve_noalloc.argtypes = [ctypes.c_void_p, ctypes.POINTER(SolveArgs), ctypes.c_int, ctypes.c_int,
+                                        ctypes.c_void_p]
         _lib = L
         return L
 

@@ -15,6 +15,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -402,4 +403,84 @@ extern "C" int cbx_flush_l2(void* buffer, size_t bytes, void* stream) {
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return fail(CBX_ERR_RUNTIME, "flush launch: %s", cudaGetErrorString(e));
     return CBX_OK;
+}
+
+// ---------------------------------------------------------------------------
+// cbx_solve_noalloc: the persistent launch with its scratch in a static array.
+//
+// Some hosts cannot call cudaMalloc while they integrate: a custom call or
+// plugin inside another framework receives only the input and output
+// buffers that framework allocated (allocating behind its memory pool would
+// break its accounting or a graph it is capturing), and a real-time loop
+// fixes its device memory at start-up.  Besides inputs and outputs, the
+// persistent kernel needs a work counter that starts at zero and a place
+// for its four iteration totals.  For those hosts both live in the array
+// below.  The driver creates it when it loads this library's device code on
+// a device, and every device that loads it keeps its 256 bytes until the
+// process exits.  The record a call uses has the same size for any batch.
+// ---------------------------------------------------------------------------
+namespace {
+constexpr int kNoAllocWords = CBX_NOALLOC_SCRATCH_BYTES / 8;
+constexpr int kNoAllocCounterWords = 1;                        // word 0: work counter
+constexpr int kNoAllocRecordWords = kNoAllocCounterWords + 4;  // words 1-4: totals
+static_assert(kNoAllocRecordWords <= kNoAllocWords, "scratch record larger than the scratch array");
+static __device__ __align__(256) unsigned long long g_noalloc_scratch[kNoAllocWords];
+
+constexpr int kNoAllocMaxDevices = 64;
+unsigned long long* g_noalloc_addr[kNoAllocMaxDevices] = {};
+std::mutex g_noalloc_mutex;
+
+// Device address of the scratch array on ``device``.  The first call for a
+// device makes that device current, asks the runtime for the address (this
+// loads the library's device code into the device's primary context) and
+// restores the previous device; later calls reuse the address.
+int noalloc_scratch(int device, unsigned long long** out) {
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (g_noalloc_addr[device]) {
+        *out = g_noalloc_addr[device];
+        return CBX_OK;
+    }
+    int prev = -1;
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    if (prev != device) {
+        cudaError_t e = cudaSetDevice(device);
+        if (e != cudaSuccess) return fail(CBX_ERR_RUNTIME, "cudaSetDevice(%d): %s", device, cudaGetErrorString(e));
+    }
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (prev >= 0 && prev != device) cudaSetDevice(prev);
+    if (e != cudaSuccess || !p)
+        return fail(CBX_ERR_RUNTIME, "cudaGetSymbolAddress of the no-alloc scratch on device %d: %s", device,
+                    cudaGetErrorString(e));
+    g_noalloc_addr[device] = static_cast<unsigned long long*>(p);
+    *out = g_noalloc_addr[device];
+    return CBX_OK;
+}
+}  // namespace
+
+extern "C" int cbx_solve_noalloc(cbx_module* module, const cbx_solve_args* args, int block, int grid,
+                                 void* stream) {
+    if (!module || !args) return fail(CBX_ERR_ARGUMENT, "null module or args");
+    if (module->device < 0 || module->device >= kNoAllocMaxDevices)
+        return fail(CBX_ERR_ARGUMENT, "cbx_solve_noalloc supports device ordinals 0-%d, got %d",
+                    kNoAllocMaxDevices - 1, module->device);
+    unsigned long long* scratch = nullptr;
+    int rc = noalloc_scratch(module->device, &scratch);
+    if (rc) return rc;
+    CUcontext cur = nullptr;
+    g_drv.cuCtxGetCurrent(&cur);
+    if (cur != module->context) {
+        rc = check_cu(g_drv.cuCtxSetCurrent(module->context), "cuCtxSetCurrent");
+        if (rc) return rc;
+    }
+    cbx_solve_args local = *args;
+    local.work_counter = scratch;
+    const bool scratch_totals = local.totals == nullptr;
+    if (scratch_totals) local.totals = scratch + kNoAllocCounterWords;
+    // The array keeps the previous call's counter and totals: clear the
+    // words this call reads before it starts, in stream order.
+    const size_t clear = sizeof(unsigned long long) * (scratch_totals ? kNoAllocRecordWords : kNoAllocCounterWords);
+    cudaError_t e = cudaMemsetAsync(scratch, 0, clear, static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) return fail(CBX_ERR_RUNTIME, "clearing the no-alloc scratch: %s", cudaGetErrorString(e));
+    return cbx_solve(module, &local, CBX_KERNEL_PERSISTENT, block, grid, stream);
 }

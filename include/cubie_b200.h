@@ -97,6 +97,35 @@ int cbx_fp32_peak_probe(int device, double* flops, float* milliseconds);
  * flush between timed launches). */
 int cbx_flush_l2(void* buffer, size_t bytes, void* stream);
 
+/* Size of the device scratch array behind cbx_solve_noalloc.  Every device
+ * that loads this library holds it until the process exits. */
+#define CBX_NOALLOC_SCRATCH_BYTES 256
+
+/* The persistent launch of cbx_solve for hosts that cannot allocate device
+ * memory while they run: a custom call or plugin inside another framework
+ * that hands it only that framework's input and output buffers, or a loop
+ * whose device memory is fixed at start-up.  No counterpart in the
+ * reference (its kernels allocate nothing themselves; Numba's launch does).
+ *
+ * Same arguments and meaning as cbx_solve with kernel = persistent, except
+ * that args->work_counter is ignored: the work counter lives in a static
+ * device array of CBX_NOALLOC_SCRATCH_BYTES bytes (a call needs 40 of them
+ * for any batch size), and the four iteration totals go there too when
+ * args->totals is NULL (to args->totals, which the caller zeroes, when it
+ * is not).  The call clears the scratch words it uses, in stream order,
+ * before the launch; the array keeps the last call's values afterwards.
+ * Calls that overlap on the GPU (on different streams, or from several
+ * threads) share the array and race: serialise them.  Rejects device
+ * ordinals of 64 and above.  Calls no cudaMalloc or cudaFree.
+ *
+ * The first call on a device looks up the array's device address with
+ * cudaGetSymbolAddress (making that device current for the lookup and then
+ * restoring the previous device), which loads this library's device code
+ * into the device's primary context: make that first call before any
+ * stream capture. */
+int cbx_solve_noalloc(cbx_module* module, const cbx_solve_args* args, int block, int grid,
+                      void* stream);
+
 #ifdef __cplusplus
 }
 #endif
