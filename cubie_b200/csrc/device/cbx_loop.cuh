@@ -432,10 +432,16 @@ __device__ __forceinline__ void run_persistent(const cbx_solve_args a) {
 
 }  // namespace cbx
 
+// Launch bounds: the block size, plus a minimum of resident blocks per SM
+// when the configuration asks for one (which caps registers per thread).
+#ifndef CBX_LAUNCH_BOUNDS
+#define CBX_LAUNCH_BOUNDS(CFG) __launch_bounds__(CFG::BLOCK)
+#endif
+
 #define CBX_DEFINE_KERNELS(CFG)                                                                     \
-    extern "C" __global__ void __launch_bounds__(CFG::BLOCK) cbx_integrate_plain(cbx_solve_args a) { \
+    extern "C" __global__ void CBX_LAUNCH_BOUNDS(CFG) cbx_integrate_plain(cbx_solve_args a) { \
         cbx::run_plain<CFG>(a);                                                                     \
     }                                                                                               \
-    extern "C" __global__ void __launch_bounds__(CFG::BLOCK) cbx_integrate_persistent(cbx_solve_args a) { \
+    extern "C" __global__ void CBX_LAUNCH_BOUNDS(CFG) cbx_integrate_persistent(cbx_solve_args a) { \
         cbx::run_persistent<CFG>(a);                                                                \
     }

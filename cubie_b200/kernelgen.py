@@ -95,6 +95,7 @@ class KernelSpec:
     # execution policy
     mixed_precision: bool = False
     block_size: int = 128
+    min_blocks_per_sm: int = 1
     dense_prediction: Optional[bool] = None
 
     @property
@@ -312,10 +313,13 @@ def generate_kernel(system: SymbolicODE, spec: KernelSpec, gen: Optional[Generat
         f"    static constexpr double DRV_INV_RESOLUTION = {_lit(spec.driver_inv_resolution)};",
         f"    static constexpr bool DRV_WRAP = {str(spec.driver_wrap).lower()};",
         f"    static constexpr int BLOCK = {int(spec.block_size)};",
+        f"    static constexpr int MIN_BLOCKS = {max(int(spec.min_blocks_per_sm), 1)};",
         f"    using Step = {STEP_TYPES[tab.kind]};",
         "};",
     ]
     lines.append("\n".join(cfg))
+    if int(spec.min_blocks_per_sm) > 1:
+        lines.append("#define CBX_LAUNCH_BOUNDS(CFG) __launch_bounds__(CFG::BLOCK, CFG::MIN_BLOCKS)")
     lines.append('#include "cbx_loop.cuh"')
     lines.append("CBX_DEFINE_KERNELS(Cfg)")
     return GeneratedKernel(source="\n".join(lines) + "\n", system=gen, spec=spec)

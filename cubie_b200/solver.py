@@ -52,7 +52,7 @@ OUTPUT_KEYS = {"output_types", "saved_state_indices", "saved_observable_indices"
                "summarised_state_indices", "summarised_observable_indices",
                "save_variables", "summarise_variables"}
 LOOP_KEYS = {"save_every", "summarise_every", "sample_summaries_every"}
-EXECUTION_KEYS = {"mixed_precision", "kernel", "block_size", "max_steps", "device", "fast_math",
+EXECUTION_KEYS = {"mixed_precision", "kernel", "block_size", "min_blocks_per_sm", "max_steps", "device", "fast_math",
                   "precision"}
 IGNORED_KEYS = {"memory_settings", "cache", "auto_memory", "lineinfo", "time_logging_level",
                 "profileCUDA", "cache_settings"}
@@ -133,6 +133,7 @@ class Solver:
         if self.kernel_kind not in ("plain", "persistent"):
             raise ValueError("kernel must be 'plain' or 'persistent'")
         self.block_size = int(execution.get("block_size", 128))
+        self.min_blocks_per_sm = int(execution.get("min_blocks_per_sm", 1))
         self.max_steps = int(execution.get("max_steps", 0))
         self.device = int(execution.get("device", 0))
         self.fast_math = bool(execution.get("fast_math", True))
@@ -361,6 +362,7 @@ class Solver:
             driver_eval_start=dm.get("eval_start", 0.0), driver_inv_resolution=dm.get("inv_resolution", 1.0),
             driver_wrap=dm.get("wrap", False),
             mixed_precision=self.mixed_precision, block_size=self.block_size,
+            min_blocks_per_sm=self.min_blocks_per_sm,
             dense_prediction=None if self.attempt_dense_prediction else False,
         )
 

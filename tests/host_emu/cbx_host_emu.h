@@ -16,7 +16,7 @@
 #define __forceinline__ inline
 #define __constant__ static
 #define __shared__ static
-#define __launch_bounds__(x)
+#define __launch_bounds__(...)
 
 using std::ceil;
 using std::fabs;
