@@ -176,6 +176,91 @@ def measured_peaks():
     return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "fallback": True}
 
 
+FHN = ["dV = V - V**3 / 3 - w + I", "dw = (V + a - b * w) / tau"]
+ADJ_T = 200.0
+
+
+def adjoint_arm(args, dev):
+    """Forward vs forward + discrete adjoint on FitzHugh-Nagumo: per-run
+    a~U[0.5,0.9], b~U[0.6,1], tau~U[8,15], I~U[0.3,0.6], (V0, w0) from
+    U[-1,1] x U[-0.5,0.5], t in [0, 200], V saved every 1.0 (201 rows),
+    DP54 rtol = atol = 1e-6 with FP32 stepping and FP64 control, loss =
+    mean((V - V_target)^2) with seeded targets, checkpoints every 64
+    accepted steps.  Gradients of 16 runs are compared with the FP64
+    forward-sensitivity reference."""
+    import torch
+    from cubie_b200 import Solver, create_ODE_system, _native
+    from cubie_b200.adjoint import AdjointIntegrator
+    n = args.adj_n
+    rng = np.random.default_rng(4)
+    p = np.stack([rng.uniform(0.5, 0.9, n), rng.uniform(0.6, 1.0, n), rng.uniform(8.0, 15.0, n),
+                  rng.uniform(0.3, 0.6, n)])
+    x0 = np.stack([rng.uniform(-1.0, 1.0, n), rng.uniform(-0.5, 0.5, n)])
+    rows = int(ADJ_T) + 1
+    target = rng.uniform(-1.0, 1.0, (rows, n))
+    sysm = create_ODE_system(FHN, states={"V": 0.0, "w": 0.0}, parameters={"a": 0.7, "b": 0.8, "tau": 12.5, "I": 0.5},
+                             precision=np.float32)
+    solver = Solver(sysm, algorithm="dormand-prince-54", rtol=1e-6, atol=1e-6, output_types=["state"],
+                    saved_state_indices=[0], save_every=1.0, mixed_precision=True, adjoint=True,
+                    device=dev.index)
+    integ = AdjointIntegrator(solver, ckpt_every=64, max_ckpts=64)
+    xi = torch.tensor(x0, device=dev, dtype=torch.float32)
+    pi = torch.tensor(p, device=dev, dtype=torch.float32)
+    tgt = torch.tensor(target, device=dev, dtype=torch.float32)
+    stream = torch.cuda.current_stream(dev)
+    flush = torch.empty(int(256e6) // 4, dtype=torch.int32, device=dev)
+    prep = solver.prepare(ADJ_T)
+    bufs = solver.allocate_outputs(prep, n, dev, torch.float32)
+    fwd_ms, tot_ms = [], []
+    for it in range(args.adj_warmup + args.adj_steps):
+        a = solver.make_args(prep, bufs, xi, pi, None, n, ADJ_T, 0.0, 0.0)
+        _native.flush_l2(flush.data_ptr(), flush.numel() * 4, stream.cuda_stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        prep["module"].launch(a, 1, solver.block_size, 0, stream.cuda_stream)
+        e1.record(stream)
+        e1.synchronize()
+        if it >= args.adj_warmup:
+            fwd_ms.append(e0.elapsed_time(e1))
+    for it in range(args.adj_warmup + args.adj_steps):
+        _native.flush_l2(flush.data_ptr(), flush.numel() * 4, stream.cuda_stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        state, status, saved = integ.forward(xi, pi, ADJ_T)
+        grad_rows = (2.0 / (rows * n)) * (state - tgt[:, None, :])
+        gi, gp = integ.backward(saved, grad_rows)
+        e1.record(stream)
+        e1.synchronize()
+        if it >= args.adj_warmup:
+            tot_ms.append(e0.elapsed_time(e1))
+    st = status.cpu().numpy()
+    # gradient check against FP64 forward sensitivities on 16 runs
+    from oracle.sensitivity import SensitivitySystem, trajectory_gradients
+    k = 16
+    g_rows = np.zeros((rows, 2, k))
+    g_rows[:, 0, :] = grad_rows[:, 0, :k].double().cpu().numpy()
+    ref_states, gy0, gpr = trajectory_gradients(SensitivitySystem(FHN, ["V", "w"], ["a", "b", "tau", "I"]),
+                                                x0[:, :k], p[:, :k], np.arange(rows, dtype=float), g_rows,
+                                                rtol=1e-11, atol=1e-11)
+    gi_h = gi[:, :k].double().cpu().numpy()
+    gp_h = gp[:, :k].double().cpu().numpy()
+    v_err = np.abs(state[:, 0, :k].double().cpu().numpy() - ref_states[:, 0, :]) / (1e-6 + 1e-6 * np.abs(ref_states[:, 0, :]))
+    f_ms, t_ms = float(np.mean(fwd_ms)), float(np.mean(tot_ms))
+    solved = float(np.mean(st == 0))
+    del flush
+    return {"workload": "FitzHugh-Nagumo, per-run a,b,tau,I; t in [0,200]; V saved every 1.0 (201 rows); DP54 "
+                        "rtol=atol=1e-6, FP32 stepping + FP64 control; loss mean((V-V_target)^2); checkpoints every 64 "
+                        "accepted steps",
+            "n_systems": n, "fwd_ms": f_ms, "fwd_plus_adjoint_ms": t_ms, "ratio": t_ms / f_ms,
+            "fwd_value": n * solved / (f_ms * 1e-3), "fwd_plus_adjoint_value": n * solved / (t_ms * 1e-3),
+            "unit": "systems/s", "status_ok_fraction": solved,
+            "grad_rel_error_vs_fp64_sensitivities": {
+                "inits": float(np.max(np.abs(gi_h - gy0)) / np.max(np.abs(gy0))),
+                "params": float(np.max(np.abs(gp_h - gpr)) / np.max(np.abs(gpr))), "runs": k},
+            "V_error_tol_units_max": float(np.max(v_err)),
+            "checkpoint_and_record_bytes": list(integ.sizes(prep))}
+
+
 def plain_wave(sysm, device: int) -> int:
     """Runs in one full resident wave of the plain kernel on this GPU."""
     from cubie_b200 import Solver, _native
@@ -328,6 +413,8 @@ def gpu_arm(args, rank: int, world: int, dist):
         peak_fp32 = _native.fp32_peak(dev.index) / 1e12
         hbm_bytes = (x0.size * 4 + mu.size * 4 + durs.size * 8 + 2 * 2 * n * 4 + n * 4)
         peaks = measured_peaks()
+        adj = adjoint_arm(args, dev) if args.adj_n > 0 else None
+        log('adjoint', adj)
         cpu = cpu_reference(per_core=args.cpu_per_core, max_steps=args.cpu_max_steps) if not args.no_cpu else None
         out = {
             "metric": "solved systems/s at matched FP64-oracle error (fwd), persistent mixed-precision path",
@@ -375,6 +462,7 @@ def gpu_arm(args, rank: int, world: int, dist):
             "plain_same_settings": {"value": n * s_frac / (s_ms * 1e-3), "ms": s_ms, "solved_fraction": s_frac,
                                     "config": "plain one-thread-per-run launch, same algorithm and precision "
                                               "settings as the headline line"},
+            "adjoint": adj,
             "cpu_baseline": cpu,
             "clocks": clocks.summary(),
         }
@@ -412,6 +500,9 @@ def main():
     ap.add_argument("--cpu-per-core", type=int, default=2)
     ap.add_argument("--cpu-max-steps", type=int, default=3000)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--adj-n", type=int, default=262144, help="FitzHugh-Nagumo adjoint leg size (0: skip)")
+    ap.add_argument("--adj-steps", type=int, default=3)
+    ap.add_argument("--adj-warmup", type=int, default=1)
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

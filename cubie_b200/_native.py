@@ -59,11 +59,27 @@ class SolveArgs(ctypes.Structure):
     ]
 
 
+class AdjointArgs(ctypes.Structure):
+    """Mirror of ``cbx_adjoint_args`` (cubie_b200/csrc/device/cbx_args.h)."""
+
+    _fields_ = [
+        ("ckpt", ctypes.c_void_p),
+        ("ckpt_count", ctypes.c_void_p),
+        ("seg", ctypes.c_void_p),
+        ("grad_state", ctypes.c_void_p),
+        ("grad_inits", ctypes.c_void_p),
+        ("grad_params", ctypes.c_void_p),
+        ("lane_words", ctypes.c_longlong),
+        ("ckpt_every", ctypes.c_int),
+        ("max_ckpts", ctypes.c_int),
+    ]
+
+
 EXPORTED = (
     "cbx_version", "cbx_last_error", "cbx_nvrtc_version", "cbx_compile", "cbx_free",
     "cbx_module_load", "cbx_module_create", "cbx_module_destroy", "cbx_kernel_info",
     "cbx_occupancy", "cbx_solve", "cbx_device_info", "cbx_fp32_peak_probe", "cbx_flush_l2",
-    "cbx_solve_noalloc",
+    "cbx_solve_noalloc", "cbx_adjoint_info", "cbx_adjoint_launch",
 )
 
 _lib = None
@@ -118,6 +134,10 @@ def lib():
         L.cbx_flush_l2.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]
         L.cbx_solve_noalloc.argtypes = [ctypes.c_void_p, ctypes.POINTER(SolveArgs), ctypes.c_int, ctypes.c_int,
                                         ctypes.c_void_p]
+        L.cbx_adjoint_info.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong),
+                                       ctypes.POINTER(ctypes.c_longlong)]
+        L.cbx_adjoint_launch.argtypes = [ctypes.c_void_p, ctypes.POINTER(SolveArgs), ctypes.POINTER(AdjointArgs),
+                                         ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
         _lib = L
         return L
 
@@ -213,6 +233,17 @@ class Module:
     def launch(self, args: SolveArgs, kernel: int, block: int, grid: int = 0, stream: int = 0) -> None:
         _check(lib().cbx_solve(self._handle, ctypes.byref(args), kernel, block, grid, ctypes.c_void_p(stream)),
                "cbx_solve")
+
+    def adjoint_sizes(self) -> tuple:
+        """(bytes of one checkpoint image, bytes of one replay record)."""
+        v, r = ctypes.c_longlong(), ctypes.c_longlong()
+        _check(lib().cbx_adjoint_info(self._handle, ctypes.byref(v), ctypes.byref(r)), "cbx_adjoint_info")
+        return v.value, r.value
+
+    def adjoint_launch(self, args: SolveArgs, adj: AdjointArgs, phase: int, block: int, grid: int = 0,
+                       stream: int = 0) -> None:
+        _check(lib().cbx_adjoint_launch(self._handle, ctypes.byref(args), ctypes.byref(adj), phase, block, grid,
+                                        ctypes.c_void_p(stream)), "cbx_adjoint_launch")
 
     def __del__(self):
         try:

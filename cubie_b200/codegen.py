@@ -252,8 +252,13 @@ class GeneratedSystem:
         return hashlib.sha256(self.source.encode()).hexdigest()[:16]
 
 
-def generate_system(system: SymbolicODE, struct_name: str = "System") -> GeneratedSystem:
-    """Return the CUDA C++ ``struct`` implementing ``system``."""
+def generate_system(system: SymbolicODE, struct_name: str = "System", second_order: bool = False) -> GeneratedSystem:
+    """Return the CUDA C++ ``struct`` implementing ``system``.
+
+    With ``second_order`` the struct also carries the contractions the
+    Rosenbrock adjoint needs, ``hvpy``: out_i = d/dy_i (v^T J(y) w) and
+    ``hvpp``: out_m = d/dp_m (v^T J(y) w), generated from the symbolic
+    second derivatives."""
     n = system.num_states
     y_map = {s: f"y[{i}]" for i, s in enumerate(system.state_symbols)}
     p_map = {s: f"p[{i}]" for i, s in enumerate(system.parameter_symbols)}
@@ -305,6 +310,21 @@ def generate_system(system: SymbolicODE, struct_name: str = "System") -> Generat
         terms = " + ".join(f"P[{k}]*v[{i}]" for k, i in pcols.get(j, [])) or "R(0)"
         ptmv_lines.append(f"        out[{j}] = {terms};")
 
+    second = []
+    if second_order:
+        w_syms = [sp.Symbol(f"_w{i}", real=True) for i in range(n)]
+        v_syms = [sp.Symbol(f"_v{i}", real=True) for i in range(n)]
+        wv_map = {**{w_syms[i]: f"w[{i}]" for i in range(n)}, **{v_syms[i]: f"v[{i}]" for i in range(n)}}
+        contraction = sum(v_syms[i] * J[i, j] * w_syms[j] for (i, j) in jac_pattern) if jac_pattern else sp.Integer(0)
+        gy = [sp.diff(contraction, ys) for ys in system.state_symbols]
+        gp = [sp.diff(contraction, ps) for ps in system.parameter_symbols]
+        body_hy, flops["hvpy"] = _emit_block([(f"out[{i}]", e) for i, e in enumerate(gy)], {**base_map, **wv_map})
+        body_hp, flops["hvpp"] = _emit_block([(f"out[{i}]", e) for i, e in enumerate(gp)], {**base_map, **wv_map})
+        second = [("hvpy(const R* __restrict__ y, const R* __restrict__ p, const R* __restrict__ d, R t, "
+                   "const R* __restrict__ w, const R* __restrict__ v, R* __restrict__ out)", body_hy),
+                  ("hvpp(const R* __restrict__ y, const R* __restrict__ p, const R* __restrict__ d, R t, "
+                   "const R* __restrict__ w, const R* __restrict__ v, R* __restrict__ out)", body_hp)]
+
     def fn(sig, body):
         body = body if body.strip() else "        (void)0;"
         return f"    template <class R>\n    static __device__ __forceinline__ void {sig}\n    {{\n{body}\n    }}\n"
@@ -333,6 +353,7 @@ def generate_system(system: SymbolicODE, struct_name: str = "System") -> Generat
               f"        {unused} (void)P;\n" + body_p),
            fn("ptmv(const R* __restrict__ P, const R* __restrict__ v, R* __restrict__ out)",
               "        (void)P; (void)v; (void)out;\n" + "\n".join(ptmv_lines)),
+           *[fn(sig, f"        {unused} (void)w; (void)v; (void)out;\n" + body) for sig, body in second],
            "};"]
     source = "\n".join(src)
     return GeneratedSystem(name=system.name, source=source, n=n,

@@ -46,4 +46,31 @@ typedef struct cbx_solve_args {
     int n_summary_rows;
 } cbx_solve_args;
 
+/* Extra arguments of the discrete-adjoint kernels (forward with
+ * checkpoints, then the reverse sweep).  The reference has no adjoint.
+ *
+ *   ckpt        [run][slot][lane_bytes / 4] 32-bit words: the complete
+ *               per-run loop state at every ckpt_every-th accepted step
+ *               (slot 0 = the state after the run is seeded);
+ *   ckpt_count  [run] int32: slots written by the forward launch;
+ *   seg         [run][ckpt_every][record_bytes]: one record per accepted
+ *               step of the segment being replayed (start state, start
+ *               time, step size, saved row), system precision;
+ *   grad_state  [n_save_rows][n_saved_states + save_time][run_stride]:
+ *               dL/d(saved state), same layout as state_out;
+ *   grad_inits  [n_states][run_stride], grad_params [n_params][run_stride]:
+ *               results (written, not accumulated).
+ */
+typedef struct cbx_adjoint_args {
+    void* ckpt;
+    int* ckpt_count;
+    void* seg;
+    const void* grad_state;
+    void* grad_inits;
+    void* grad_params;
+    long long lane_words;       /* lane_bytes / 4 as reported by the module (a multiple of 4) */
+    int ckpt_every;
+    int max_ckpts;
+} cbx_adjoint_args;
+
 #endif /* CBX_ARGS_H */

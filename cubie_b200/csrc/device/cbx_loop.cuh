@@ -184,9 +184,18 @@ __device__ __forceinline__ void lane_begin(Lane<Cfg>& L, const cbx_solve_args a,
     Step::init(L.ps);
 }
 
+// Observer of accepted steps (the adjoint's segment recorder); the default
+// observes nothing and compiles away.
+struct NoHook {
+    static constexpr bool ACTIVE = false;
+};
+
 // One pass of the main loop body.  Returns true when the run is finished.
-template <class Cfg>
-__device__ __forceinline__ bool lane_iterate(Lane<Cfg>& L, const cbx_solve_args a) {
+// ``hook->accepted(L, t, h, row)`` sees every accepted step before the state
+// is updated: the step's start time and size exactly as the step function
+// received them, and the output row saved at its end (-1 if none).
+template <class Cfg, class Hook = NoHook>
+__device__ __forceinline__ bool lane_iterate(Lane<Cfg>& L, const cbx_solve_args a, Hook* hook = nullptr) {
     using R = typename Cfg::R;
     using C = typename Cfg::C;
     using Step = typename Cfg::Step;
@@ -288,6 +297,7 @@ __device__ __forceinline__ bool lane_iterate(Lane<Cfg>& L, const cbx_solve_args 
     if (L.irrecoverable) L.status |= L.iteration_status;
     if (accept) L.iteration_status = 0;
     if (accept) {
+        if constexpr (Hook::ACTIVE) hook->accepted(L, R(L.tp), R(dt_eff), do_save ? L.save_idx : -1);
         L.t = t_proposal;
         L.tp = C(L.t);
         if (Cfg::MIXED) {

@@ -27,6 +27,12 @@ struct cbx_module {
     CUfunction fn[2];
     int device;
     int sm_count;
+    // discrete-adjoint kernels, resolved on first use (modules generated
+    // without them have neither)
+    CUfunction adj[2];
+    size_t lane_bytes;
+    size_t record_bytes;
+    bool adj_resolved;
 };
 
 namespace {
@@ -54,6 +60,7 @@ struct DriverApi {
     CBX_DRV(cuLaunchKernel)
     CBX_DRV(cuGetErrorName)
     CBX_DRV(cuGetErrorString)
+    CBX_DRV(cuModuleGetGlobal)
 #undef CBX_DRV
 };
 
@@ -90,6 +97,12 @@ bool load_driver() {
     CBX_SYM(cuGetErrorName)
     CBX_SYM(cuGetErrorString)
 #undef CBX_SYM
+    // versioned entry point: the 64-bit size variant behind cuda.h's macro
+    g_drv.cuModuleGetGlobal = reinterpret_cast<decltype(g_drv.cuModuleGetGlobal)>(dlsym(h, "cuModuleGetGlobal_v2"));
+    if (!g_drv.cuModuleGetGlobal) {
+        g_drv.failed = true;
+        return false;
+    }
     g_drv.loaded = true;
     return true;
 }
@@ -335,6 +348,89 @@ int cbx_device_info(int device, int* sm_count, int* cc_major, int* cc_minor) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Discrete adjoint launches.
+// ---------------------------------------------------------------------------
+namespace {
+int resolve_adjoint(cbx_module* m) {
+    if (m->adj_resolved) return CBX_OK;
+    CUdeviceptr probe = 0;
+    size_t bytes = 0;
+    if (g_drv.cuModuleGetGlobal(&probe, &bytes, m->module, "cbx_lane_probe") != CUDA_SUCCESS)
+        return fail(CBX_ERR_ARGUMENT, "module was generated without the adjoint kernels");
+    CUdeviceptr probe2 = 0;
+    size_t rbytes = 0;
+    if (g_drv.cuModuleGetGlobal(&probe2, &rbytes, m->module, "cbx_seg_record_probe") != CUDA_SUCCESS)
+        return fail(CBX_ERR_ARGUMENT, "module was generated without the adjoint kernels");
+    const char* names[2] = {"cbx_adjoint_forward", "cbx_adjoint_backward"};
+    for (int k = 0; k < 2; ++k) {
+        int rc = check_cu(g_drv.cuModuleGetFunction(&m->adj[k], m->module, names[k]), names[k]);
+        if (rc) return rc;
+    }
+    m->lane_bytes = bytes;
+    m->record_bytes = rbytes;
+    m->adj_resolved = true;
+    return CBX_OK;
+}
+}  // namespace
+
+extern "C" int cbx_adjoint_info(cbx_module* module, long long* lane_bytes, long long* record_bytes) {
+    if (!module || !lane_bytes || !record_bytes) return fail(CBX_ERR_ARGUMENT, "null module or output pointer");
+    if (!load_driver()) return fail(CBX_ERR_NO_DEVICE, "CUDA driver library is not available");
+    int rc = resolve_adjoint(module);
+    if (rc) return rc;
+    *lane_bytes = (long long)module->lane_bytes;
+    *record_bytes = (long long)module->record_bytes;
+    return CBX_OK;
+}
+
+extern "C" int cbx_adjoint_launch(cbx_module* module, const cbx_solve_args* args, const cbx_adjoint_args* adj,
+                                  int phase, int block, int grid, void* stream) {
+    if (!module || !args || !adj) return fail(CBX_ERR_ARGUMENT, "null module, args or adjoint args");
+    if (phase != 0 && phase != 1) return fail(CBX_ERR_ARGUMENT, "phase must be 0 (forward) or 1 (backward)");
+    if (block <= 0 || block > 1024 || (block % 32) != 0)
+        return fail(CBX_ERR_ARGUMENT, "block size %d must be a positive multiple of 32 <= 1024", block);
+    if (args->n_runs < 0 || args->run_stride < args->n_runs)
+        return fail(CBX_ERR_ARGUMENT, "run_stride (%lld) must be >= n_runs (%lld)", args->run_stride, args->n_runs);
+    if (!args->inits || !args->work_counter)
+        return fail(CBX_ERR_ARGUMENT, "inits and a zeroed work_counter are required");
+    if (!adj->ckpt || !adj->ckpt_count || adj->ckpt_every < 1 || adj->max_ckpts < 1)
+        return fail(CBX_ERR_ARGUMENT, "checkpoint buffers, ckpt_every >= 1 and max_ckpts >= 1 are required");
+    if (phase == 0 && !args->status_out) return fail(CBX_ERR_ARGUMENT, "status_out is required");
+    if (phase == 1 && (!adj->seg || !adj->grad_inits))
+        return fail(CBX_ERR_ARGUMENT, "seg and grad_inits are required for the backward sweep");
+    if (!load_driver()) return fail(CBX_ERR_NO_DEVICE, "CUDA driver library is not available");
+    CUcontext cur = nullptr;
+    g_drv.cuCtxGetCurrent(&cur);
+    if (cur != module->context) {
+        int rc = check_cu(g_drv.cuCtxSetCurrent(module->context), "cuCtxSetCurrent");
+        if (rc) return rc;
+    }
+    int rc = resolve_adjoint(module);
+    if (rc) return rc;
+    if ((size_t)adj->lane_words * 4 < module->lane_bytes)
+        return fail(CBX_ERR_ARGUMENT, "lane_words (%lld) is smaller than the module's lane image (%zu bytes)",
+                    adj->lane_words, module->lane_bytes);
+    if (args->n_runs == 0) return CBX_OK;
+    CUfunction f = module->adj[phase];
+    long long g = grid;
+    if (g <= 0) {
+        int per_sm = 0;
+        if (g_drv.cuOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, f, block, 0) != CUDA_SUCCESS || per_sm <= 0)
+            per_sm = 1;
+        g = (long long)per_sm * module->sm_count;
+        long long needed = (args->n_runs + block - 1) / block;
+        if (g > needed) g = needed;
+    }
+    if (g > 2147483647LL) return fail(CBX_ERR_ARGUMENT, "grid too large");
+    cbx_solve_args la = *args;
+    cbx_adjoint_args lg = *adj;
+    void* params[] = {&la, &lg};
+    return check_cu(g_drv.cuLaunchKernel(f, (unsigned)g, 1, 1, (unsigned)block, 1, 1, 0,
+                                         static_cast<CUstream>(stream), params, nullptr),
+                    "cuLaunchKernel");
+}
 
 // ---------------------------------------------------------------------------
 // Fixed utility kernels (compiled by nvcc for sm_100a with the library).

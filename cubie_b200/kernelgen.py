@@ -24,7 +24,7 @@ import numpy as np
 
 from .codegen import GeneratedSystem, generate_system
 from .outputs import SummaryPlan
-from .symbolic import SymbolicODE
+from .symbolic import TIME, SymbolicODE
 from .tableaus import DIRK, ERK, FIRK, ROSENBROCK, Tableau
 
 ALGO_IDS = {ERK: "cbx::ALGO_ERK", DIRK: "cbx::ALGO_DIRK", FIRK: "cbx::ALGO_FIRK", ROSENBROCK: "cbx::ALGO_ROSENBROCK"}
@@ -32,6 +32,7 @@ STEP_TYPES = {ERK: "cbx::ErkStep<Cfg>", DIRK: "cbx::DirkStep<Cfg>", FIRK: "cbx::
               ROSENBROCK: "cbx::RosenbrockStep<Cfg>"}
 LIN_IDS = {"minimal_residual": "cbx::LIN_MR", "steepest_descent": "cbx::LIN_SD",
            "bicgstab": "cbx::LIN_BICGSTAB", "gmres": "cbx::LIN_GMRES"}
+ADJOINT_FAMILIES = {ERK, ROSENBROCK}
 CTRL_IDS = {"fixed": "cbx::CTRL_FIXED", "i": "cbx::CTRL_I", "pi": "cbx::CTRL_PI",
             "pid": "cbx::CTRL_PID", "gustafsson": "cbx::CTRL_GUSTAFSSON"}
 
@@ -97,6 +98,8 @@ class KernelSpec:
     block_size: int = 128
     min_blocks_per_sm: int = 1
     dense_prediction: Optional[bool] = None
+    # discrete adjoint kernels (forward with checkpoints, reverse sweep)
+    adjoint: bool = False
 
     @property
     def adaptive(self) -> bool:
@@ -199,7 +202,7 @@ class GeneratedKernel:
 
 def generate_kernel(system: SymbolicODE, spec: KernelSpec, gen: Optional[GeneratedSystem] = None) -> GeneratedKernel:
     """Return the complete CUDA translation unit for ``spec``."""
-    gen = gen or generate_system(system)
+    gen = gen or generate_system(system, second_order=spec.adjoint and spec.tableau.kind == ROSENBROCK)
     tab = spec.tableau
     n = system.num_states
     rtype = "float" if np.dtype(spec.precision) == np.float32 else "double"
@@ -322,4 +325,13 @@ def generate_kernel(system: SymbolicODE, spec: KernelSpec, gen: Optional[Generat
         lines.append("#define CBX_LAUNCH_BOUNDS(CFG) __launch_bounds__(CFG::BLOCK, CFG::MIN_BLOCKS)")
     lines.append('#include "cbx_loop.cuh"')
     lines.append("CBX_DEFINE_KERNELS(Cfg)")
+    if spec.adjoint:
+        if tab.kind not in ADJOINT_FAMILIES:
+            raise NotImplementedError(f"no discrete adjoint for the {tab.kind} family "
+                                      f"(available: {sorted(ADJOINT_FAMILIES)})")
+        if tab.kind == ROSENBROCK and (system.num_drivers > 0 or any(
+                TIME in e.free_symbols for e in system.rhs_expressions())):
+            raise NotImplementedError("the Rosenbrock adjoint needs an autonomous system without drivers")
+        lines.append('#include "cbx_adjoint.cuh"')
+        lines.append("CBX_DEFINE_ADJOINT_KERNELS(Cfg)")
     return GeneratedKernel(source="\n".join(lines) + "\n", system=gen, spec=spec)

@@ -53,7 +53,7 @@ OUTPUT_KEYS = {"output_types", "saved_state_indices", "saved_observable_indices"
                "save_variables", "summarise_variables"}
 LOOP_KEYS = {"save_every", "summarise_every", "sample_summaries_every"}
 EXECUTION_KEYS = {"mixed_precision", "kernel", "block_size", "min_blocks_per_sm", "max_steps", "device", "fast_math",
-                  "precision"}
+                  "precision", "adjoint"}
 IGNORED_KEYS = {"memory_settings", "cache", "auto_memory", "lineinfo", "time_logging_level",
                 "profileCUDA", "cache_settings"}
 RENAMED = {"dt_save": "save_every", "dt_summarise": "summarise_every",
@@ -134,6 +134,7 @@ class Solver:
             raise ValueError("kernel must be 'plain' or 'persistent'")
         self.block_size = int(execution.get("block_size", 128))
         self.min_blocks_per_sm = int(execution.get("min_blocks_per_sm", 1))
+        self.adjoint = bool(execution.get("adjoint", False))
         self.max_steps = int(execution.get("max_steps", 0))
         self.device = int(execution.get("device", 0))
         self.fast_math = bool(execution.get("fast_math", True))
@@ -362,13 +363,23 @@ class Solver:
             driver_eval_start=dm.get("eval_start", 0.0), driver_inv_resolution=dm.get("inv_resolution", 1.0),
             driver_wrap=dm.get("wrap", False),
             mixed_precision=self.mixed_precision, block_size=self.block_size,
-            min_blocks_per_sm=self.min_blocks_per_sm,
+            min_blocks_per_sm=self.min_blocks_per_sm, adjoint=self.adjoint,
             dense_prediction=None if self.attempt_dense_prediction else False,
         )
 
+    def _generate(self, spec: KernelSpec):
+        """Kernel source for ``spec``; the symbolic system part (SymPy CSE,
+        the costly step) is generated once per solver."""
+        second = bool(spec.adjoint and spec.tableau.kind == "rosenbrock")
+        cache = self.__dict__.setdefault("_system_code", {})
+        gen = cache.get(second)
+        if gen is None:
+            gen = cache[second] = generate_system(self.system, second_order=second)
+        return generate_kernel(self.system, spec, gen=gen)
+
     def module_for(self, spec: KernelSpec):
         """Compile (or fetch) the NVRTC module for ``spec`` on this device."""
-        gk = generate_kernel(self.system, spec)
+        gk = self._generate(spec)
         key = (gk.key, self.device)
         mod = _MODULE_CACHE.get(key)
         if mod is None:
@@ -463,6 +474,12 @@ class Solver:
         sizes for a launch."""
         if duration <= 0:
             raise ValueError("duration must be positive")
+        key = None
+        if interp is None:
+            key = (float(duration), float(settling_time), float(t0), durations is None, bool(load))
+            hit = self.__dict__.setdefault("_prepared", {}).get(key)
+            if hit is not None:
+                return hit
         timing = self._timing(float(duration))
         if durations is not None and (timing["save_regularly"] or timing["summarise_regularly"]):
             raise ValueError("per-run durations need end-of-run saving only (no save_every or summaries)")
@@ -471,15 +488,18 @@ class Solver:
         if load:
             mod, gk = self.module_for(spec)
         else:
-            mod, gk = None, generate_kernel(self.system, spec)
+            mod, gk = None, self._generate(spec)
         p = self.precision
         n_save = output_length(duration, timing["save_every"], timing["save_last"], p) if timing["time_domain"] else 0
         n_summ = summaries_length(duration, timing["sample_every"], timing["samples_per_summary"], p) \
             if timing["summaries"] else 0
         save_stop = save_stop_time(duration, settling_time, t0, timing["save_every"], p)
         summ_stop = summary_stop_time(duration, settling_time, t0, timing["sample_every"], p)
-        return dict(timing=timing, spec=spec, module=mod, gen=gk, n_save=n_save, n_summ=n_summ,
+        prep = dict(timing=timing, spec=spec, module=mod, gen=gk, n_save=n_save, n_summ=n_summ,
                     save_stop=save_stop, summary_stop=summ_stop)
+        if key is not None:
+            self._prepared[key] = prep
+        return prep
 
     def run(self, inits: np.ndarray, params: np.ndarray, interp=None, duration: float = 1.0,
             settling_time: float = 0.0, t0: float = 0.0, nan_error_trajectories: bool = True,

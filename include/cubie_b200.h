@@ -97,6 +97,28 @@ int cbx_fp32_peak_probe(int device, double* flops, float* milliseconds);
  * flush between timed launches). */
 int cbx_flush_l2(void* buffer, size_t bytes, void* stream);
 
+/* Discrete adjoint (no counterpart in the reference, which cannot
+ * differentiate its integrations).  For a module generated with the
+ * adjoint kernels (explicit Runge-Kutta and Rosenbrock tableaus):
+ *
+ * cbx_adjoint_info reports the size of one per-run checkpoint image and of
+ * one replay record (both multiples of 16 bytes); size adj->ckpt as
+ * n_runs * max_ckpts * lane_bytes and adj->seg as
+ * n_runs * ckpt_every * record_bytes, both 16-byte aligned, and pass
+ * adj->lane_words = lane_bytes / 4.
+ *
+ * cbx_adjoint_launch with phase 0 integrates like cbx_solve's persistent
+ * kernel (same outputs) and stores a checkpoint every adj->ckpt_every
+ * accepted steps; a run needing more than adj->max_ckpts checkpoints stops
+ * with status bit 32.  Phase 1, with the same args, the checkpoints of
+ * phase 0, dL/d(saved state) in adj->grad_state and args->work_counter
+ * zeroed again, writes dL/d(initial state) and dL/d(parameters) for every
+ * run, holding the accepted step sizes fixed.  Both are asynchronous on
+ * ``stream``; grid = 0 picks a resident grid. */
+int cbx_adjoint_info(cbx_module* module, long long* lane_bytes, long long* record_bytes);
+int cbx_adjoint_launch(cbx_module* module, const cbx_solve_args* args, const cbx_adjoint_args* adj,
+                       int phase, int block, int grid, void* stream);
+
 /* Size of the device scratch array behind cbx_solve_noalloc.  Every device
  * that loads this library holds it until the process exits. */
 #define CBX_NOALLOC_SCRATCH_BYTES 256

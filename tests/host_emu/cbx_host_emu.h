@@ -9,6 +9,7 @@
 #include <cmath>
 #include <cstddef>
 #include <cstdint>
+#include <cstring>
 
 #define __device__
 #define __host__
@@ -29,6 +30,19 @@ using std::pow;
 using std::sqrt;
 inline float sqrtf(float v) { return std::sqrt(v); }
 inline float powf(float a, float b) { return std::pow(a, b); }
+
+struct float4 {
+    float x, y, z, w;
+};
+inline float4 make_float4(float x, float y, float z, float w) { return float4{x, y, z, w}; }
+struct uint4 {
+    unsigned x, y, z, w;
+};
+inline uint4 make_uint4(unsigned x, unsigned y, unsigned z, unsigned w) { return uint4{x, y, z, w}; }
+struct double2 {
+    double x, y;
+};
+inline double2 make_double2(double x, double y) { return double2{x, y}; }
 
 struct cbx_dim3 {
     unsigned x, y, z;

@@ -36,6 +36,23 @@ extern "C" void emu_launch(cbx_solve_args* a, int kernel, int grid, int block) {
 }
 """
 
+ADJOINT_DRIVER = r"""
+extern "C" void emu_adjoint(cbx_solve_args* a, cbx_adjoint_args* g, int phase, int grid, int block) {
+    blockDim = {(unsigned)block, 1, 1};
+    gridDim = {(unsigned)grid, 1, 1};
+    for (int b = 0; b < grid; ++b) {
+        for (int t = 0; t < block; ++t) {
+            blockIdx = {(unsigned)b, 0, 0};
+            threadIdx = {(unsigned)t, 0, 0};
+            if (phase == 0) cbx_adjoint_forward(*a, *g);
+            else cbx_adjoint_backward(*a, *g);
+        }
+    }
+}
+extern "C" long long emu_lane_bytes() { return (long long)sizeof(cbx_lane_probe); }
+extern "C" long long emu_record_bytes() { return (long long)sizeof(cbx_seg_record_probe); }
+"""
+
 _cache = {}
 
 
@@ -51,12 +68,16 @@ def compile_emulated(source: str):
     src = d / f"{key}.cpp"
     so = d / f"{key}.so"
     if not so.exists():
-        src.write_text(source + DRIVER)
+        src.write_text(source + DRIVER + (ADJOINT_DRIVER if "CBX_DEFINE_ADJOINT_KERNELS" in source else ""))
         cmd = ["g++", "-O1", "-std=c++17", "-shared", "-fPIC", "-include", str(HERE / "cbx_host_emu.h"),
                f"-I{DEVICE}", "-x", "c++", str(src), "-o", str(so)]
         subprocess.run(cmd, check=True, capture_output=True, text=True)
     lib = ctypes.CDLL(str(so))
     lib.emu_launch.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    if "CBX_DEFINE_ADJOINT_KERNELS" in source:
+        lib.emu_adjoint.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        lib.emu_lane_bytes.restype = ctypes.c_longlong
+        lib.emu_record_bytes.restype = ctypes.c_longlong
     _cache[key] = lib
     return lib
 
@@ -118,3 +139,60 @@ def run_emulated(solver, inits, params, duration, settling_time=0.0, t0=0.0, ker
     bufs["n_save"] = n_save
     bufs["n_summ"] = n_summ
     return bufs
+
+
+def run_emulated_adjoint(solver, inits, params, duration, grad_state_fn, ckpt_every=64, max_ckpts=64):
+    """Forward with checkpoints and the reverse sweep of the adjoint kernels
+    on the CPU.  ``grad_state_fn(state)`` returns dL/d(state rows) for the
+    forward's state output.  Returns (state, status, grad_inits, grad_params)."""
+    from cubie_b200 import _native
+    prep = solver.prepare(duration, load=False)
+    spec = prep["spec"]
+    lib = compile_emulated(prep["gen"].source)
+    p = solver.precision
+    n_runs = inits.shape[1]
+    n = inits.shape[0]
+    inits = np.ascontiguousarray(inits, dtype=p)
+    params = np.ascontiguousarray(params, dtype=p) if params.size else np.zeros((1, n_runs), p)
+    npar = solver.system.num_parameters
+    n_save = prep["n_save"]
+    width = (len(spec.saved_state_indices) if spec.save_state else 0) + (1 if spec.save_time else 0)
+    state = np.zeros((n_save, width, n_runs), p)
+    status = np.zeros((n_runs,), np.int32)
+    work = np.zeros((2,), np.uint64)
+    lane = int(lib.emu_lane_bytes())
+    words = lane // 4
+    ckpt = np.zeros((n_runs * max_ckpts * words,), np.uint32)
+    count = np.zeros((n_runs,), np.int32)
+    seg = np.zeros((ckpt_every * n_runs * int(lib.emu_record_bytes()) // 8 + 2,), np.float64)
+    gi = np.zeros((n, n_runs), p)
+    gp = np.zeros((max(npar, 1), n_runs), p)
+
+    a = _native.SolveArgs()
+    a.inits = inits.ctypes.data
+    a.params = params.ctypes.data
+    a.state_out = state.ctypes.data
+    a.status_out = status.ctypes.data
+    a.work_counter = work.ctypes.data
+    a.n_runs = a.run_stride = n_runs
+    a.max_steps = int(solver.max_steps)
+    a.duration = float(duration)
+    a.save_stop = float(prep["save_stop"])
+    a.summary_stop = float(prep["summary_stop"])
+    a.n_save_rows = int(n_save)
+    a.n_summary_rows = int(prep["n_summ"])
+    g = _native.AdjointArgs()
+    g.ckpt = ckpt.ctypes.data
+    g.ckpt_count = count.ctypes.data
+    g.lane_words = words
+    g.ckpt_every = ckpt_every
+    g.max_ckpts = max_ckpts
+    lib.emu_adjoint(ctypes.byref(a), ctypes.byref(g), 0, 1, 32)
+    grad_state = np.ascontiguousarray(grad_state_fn(state), dtype=p)
+    g.seg = seg.ctypes.data
+    g.grad_state = grad_state.ctypes.data
+    g.grad_inits = gi.ctypes.data
+    g.grad_params = gp.ctypes.data
+    work[:] = 0
+    lib.emu_adjoint(ctypes.byref(a), ctypes.byref(g), 1, 1, 32)
+    return state, status, gi, gp[:npar]
