@@ -12,6 +12,6 @@ reference's own kernels run on the CPU under Numba's CUDA simulator
 DifferentialEquations.jl golden vectors (``tests/golden/make_julia_fixture.py``).
 """
 
-from .ode_oracle import OracleSystem, integrate, TABLEAUS
+from .ode_oracle import DriverTable, OracleSystem, integrate, TABLEAUS
 
-__all__ = ["OracleSystem", "integrate", "TABLEAUS"]
+__all__ = ["DriverTable", "OracleSystem", "integrate", "TABLEAUS"]

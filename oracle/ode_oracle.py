@@ -191,13 +191,16 @@ class OracleSystem:
     SymPy-generated numpy functions over a batch of runs."""
 
     def __init__(self, equations: Sequence[str], states: Sequence[str], parameters: Sequence[str] = (),
-                 constants: Optional[Dict[str, float]] = None, observables: Sequence[str] = ()):
+                 constants: Optional[Dict[str, float]] = None, observables: Sequence[str] = (),
+                 drivers: Sequence[str] = ()):
         constants = constants or {}
         self.states = list(states)
         self.parameters = list(parameters)
         self.observables = list(observables)
+        self.drivers = list(drivers)
+        self.driver_table: Optional["DriverTable"] = None
         t = sp.Symbol("t", real=True)
-        table = {nm: sp.Symbol(nm, real=True) for nm in self.states + self.parameters}
+        table = {nm: sp.Symbol(nm, real=True) for nm in self.states + self.parameters + self.drivers}
         table.update({k: sp.Float(v, 17) for k, v in constants.items()})
         table["t"] = t
         aux = {}
@@ -216,13 +219,27 @@ class OracleSystem:
         self.n = len(self.states)
         ys = [table[s] for s in self.states]
         ps = [table[p] for p in self.parameters]
+        ds = [table[d] for d in self.drivers]
+        dds = [sp.Symbol(f"_ddot_{d}", real=True) for d in self.drivers]
         f = [derivs[s] for s in self.states]
         J = sp.Matrix(f).jacobian(sp.Matrix(ys))
-        args = (t, ys, ps)
+        args = (t, ys, ps, ds)
         self._f = sp.lambdify(args, f, "numpy")
         self._J = sp.lambdify(args, J.tolist(), "numpy")
-        self._dt = sp.lambdify(args, [sp.diff(e, t) for e in f], "numpy")
+        # time derivative with the driver chain rule (time_derivative.py:51)
+        dfdt = [sp.diff(e, t) + sum((sp.diff(e, d) * dd for d, dd in zip(ds, dds)), sp.Integer(0)) for e in f]
+        self._dt = sp.lambdify((t, ys, ps, ds, dds), dfdt, "numpy")
         self._obs = sp.lambdify(args, [table[o] for o in self.observables], "numpy") if self.observables else None
+
+    def _drv(self, t, B, dtype, derivative=False):
+        """Driver values (or time derivatives) at ``t`` for every run."""
+        if not self.drivers:
+            return []
+        if self.driver_table is None:
+            raise ValueError("the system has drivers: set ``driver_table`` first")
+        tt = np.broadcast_to(np.asarray(t, dtype=dtype), (B,))
+        vals = self.driver_table.evaluate(tt, derivative)
+        return [vals[:, k] for k in range(vals.shape[1])]
 
     @staticmethod
     def _stack(vals, B, dtype):
@@ -231,24 +248,73 @@ class OracleSystem:
     def f(self, t, Y, P):
         B = Y.shape[0]
         dtype = Y.dtype
-        return self._stack(self._f(t, [Y[:, i] for i in range(self.n)], [P[:, j] for j in range(P.shape[1])]), B, dtype)
+        return self._stack(self._f(t, [Y[:, i] for i in range(self.n)], [P[:, j] for j in range(P.shape[1])],
+                                   self._drv(t, B, dtype)), B, dtype)
 
     def jac(self, t, Y, P):
         B = Y.shape[0]
         dtype = Y.dtype
-        rows = self._J(t, [Y[:, i] for i in range(self.n)], [P[:, j] for j in range(P.shape[1])])
+        rows = self._J(t, [Y[:, i] for i in range(self.n)], [P[:, j] for j in range(P.shape[1])],
+                       self._drv(t, B, dtype))
         return np.stack([self._stack(r, B, dtype) for r in rows], axis=1)
 
     def dfdt(self, t, Y, P):
         B = Y.shape[0]
-        return self._stack(self._dt(t, [Y[:, i] for i in range(self.n)], [P[:, j] for j in range(P.shape[1])]),
+        return self._stack(self._dt(t, [Y[:, i] for i in range(self.n)], [P[:, j] for j in range(P.shape[1])],
+                                    self._drv(t, B, Y.dtype), self._drv(t, B, Y.dtype, derivative=True)),
                            B, Y.dtype)
 
     def obs(self, t, Y, P):
         if self._obs is None:
             return np.zeros((Y.shape[0], 0), Y.dtype)
-        return self._stack(self._obs(t, [Y[:, i] for i in range(self.n)], [P[:, j] for j in range(P.shape[1])]),
-                           Y.shape[0], Y.dtype)
+        B = Y.shape[0]
+        return self._stack(self._obs(t, [Y[:, i] for i in range(self.n)], [P[:, j] for j in range(P.shape[1])],
+                                     self._drv(t, B, Y.dtype)), B, Y.dtype)
+
+
+class DriverTable:
+    """Piecewise-polynomial drivers from a coefficient table
+    ``[segment, driver, power]``, evaluated as the reference's device
+    helpers do (array_interpolator.py:437-550): scaled time
+    (t - start) / period with start = t0 - period for zero-padded clamped
+    inputs, segment = floor (modulo the segment count when wrapping,
+    clamped to the table otherwise), Horner in tau, zero outside the
+    window when not wrapping; all in the working precision."""
+
+    def __init__(self, coefficients, period, t0, wrap, padded, precision):
+        p = np.dtype(precision).type
+        self.p = p
+        self.c = np.asarray(coefficients, dtype=p)
+        self.nseg = self.c.shape[0]
+        self.order = self.c.shape[2] - 1
+        res = p(period)
+        self.inv = p(p(1.0) / res)
+        self.start = p(p(t0) - (res if padded else p(0.0)))
+        self.wrap = bool(wrap)
+
+    def evaluate(self, t, derivative=False):
+        p = self.p
+        scaled = (np.asarray(t, dtype=p) - self.start) * self.inv
+        fl = np.floor(scaled)
+        idx = fl.astype(np.int64)
+        if self.wrap:
+            seg = np.mod(idx, self.nseg)
+            tau = (scaled - fl).astype(p)
+            ok = np.ones(scaled.shape, bool)
+        else:
+            ok = (scaled >= 0) & (scaled <= self.nseg)
+            seg = np.clip(idx, 0, self.nseg - 1)
+            tau = (scaled - seg.astype(p)).astype(p)
+        c = self.c[seg]
+        acc = np.zeros((scaled.shape[0], self.c.shape[1]), p)
+        if derivative:
+            for k in range(self.order, 0, -1):
+                acc = acc * tau[:, None] + p(k) * c[:, :, k]
+            acc = acc * self.inv
+        else:
+            for k in range(self.order, -1, -1):
+                acc = acc * tau[:, None] + c[:, :, k]
+        return np.where(ok[:, None], acc, p(0))
 
 
 # ---------------------------------------------------------------------------

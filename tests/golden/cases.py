@@ -18,6 +18,10 @@ VDP = dict(
     equations=["dx = y", "dy = mu * (1 - x**2) * y - x"],
     states=["x", "y"], parameters=["mu"], constants={},
 )
+DRIVEN = dict(
+    equations=["dx = v", "dv = -k * x - c * v + F"],
+    states=["x", "v"], parameters=["k", "c"], constants={}, drivers=["F"],
+)
 FHN = dict(
     equations=["dV = V - V**3 / 3 - w + I", "dw = (V + a - b * w) / tau"],
     states=["V", "w"], parameters=["a", "b", "tau", "I"], constants={},
@@ -35,6 +39,13 @@ def vdp_inputs(n, seed, mus):
     rng = np.random.default_rng(seed)
     x0 = rng.uniform(-2.0, 2.0, (2, n))
     return x0, np.asarray(mus, dtype=float)[None, :]
+
+
+def driven_inputs(n, seed):
+    rng = np.random.default_rng(seed)
+    x0 = rng.uniform(-1.0, 1.0, (2, n))
+    p = np.stack([rng.uniform(2.0, 20.0, n), rng.uniform(0.1, 2.0, n)])
+    return x0, p
 
 
 def fhn_inputs(n, seed):
@@ -99,6 +110,24 @@ CASES = {
                                kwargs=dict(rtol=1e-6, atol=1e-6, save_every=1.0, summarise_every=20.0,
                                            sample_summaries_every=0.5,
                                            output_types=["state", "time", "peaks[3]", "std", "rms", "min"])),
+    "driven_dp54_clamped_f64": dict(system=DRIVEN, algorithm="dormand-prince-54", precision="float64",
+                                    inputs=("driven", 4, 13), duration=3.0,
+                                    drivers=dict(seed=21, n_samples=16, period=0.2, t0=0.1, order=3, wrap=False,
+                                                 boundary_condition="clamped"),
+                                    kwargs=dict(rtol=1e-8, atol=1e-8, save_every=0.25,
+                                                output_types=["state", "time"])),
+    "driven_dp54_periodic_f32": dict(system=DRIVEN, algorithm="dormand-prince-54", precision="float32",
+                                     inputs=("driven", 4, 14), duration=4.0,
+                                     drivers=dict(seed=22, n_samples=11, period=0.3, t0=0.0, order=3, wrap=True,
+                                                  boundary_condition="periodic"),
+                                     kwargs=dict(rtol=1e-6, atol=1e-6, save_every=0.5,
+                                                 output_types=["state", "time"])),
+    "driven_ros3p_clamped_f64": dict(system=DRIVEN, algorithm="ros3p", precision="float64",
+                                     inputs=("driven", 4, 15), duration=3.0,
+                                     drivers=dict(seed=23, n_samples=16, period=0.2, t0=0.1, order=3, wrap=False,
+                                                  boundary_condition="clamped"),
+                                     kwargs=dict(rtol=1e-7, atol=1e-7, save_every=0.25,
+                                                 output_types=["state", "time", "iteration_counters"])),
     "lorenz_step_too_small_f32": dict(system=LORENZ, algorithm="dormand-prince-54", precision="float32",
                                       inputs=("lorenz", 2, 12), duration=1.0,
                                       kwargs=dict(rtol=1e-12, atol=1e-14, dt=0.01, dt_min=0.005, dt_max=0.1,
@@ -114,4 +143,23 @@ def case_inputs(case):
         return vdp_inputs(case["inputs"][1], case["inputs"][2], case["inputs"][3])
     if kind == "fhn":
         return fhn_inputs(case["inputs"][1], case["inputs"][2])
+    if kind == "driven":
+        return driven_inputs(case["inputs"][1], case["inputs"][2])
     raise KeyError(kind)
+
+
+def case_drivers(case):
+    """The drivers dictionary of a case (reference ``solve(drivers=...)``
+    format), or None."""
+    spec = case.get("drivers")
+    if spec is None:
+        return None
+    rng = np.random.default_rng(spec["seed"])
+    out = {"driver_sample_period": spec["period"], "t0": spec["t0"], "order": spec["order"],
+           "wrap": spec["wrap"], "boundary_condition": spec["boundary_condition"]}
+    for name in case["system"]["drivers"]:
+        samples = rng.uniform(-1.0, 1.0, spec["n_samples"])
+        if spec["boundary_condition"] == "periodic":
+            samples[-1] = samples[0]
+        out[name] = samples
+    return out

@@ -31,19 +31,20 @@ WORKER = r"""
 import json, sys, time
 import numpy as np
 sys.path.insert(0, {here!r})
-from cases import CASES, case_inputs
+from cases import CASES, case_inputs, case_drivers
 from cubie import create_ODE_system, Solver
 name = {name!r}
 case = CASES[name]
 sysd = case["system"]
 prec = np.dtype(case["precision"]).type
+drivers = case_drivers(case)
 system = create_ODE_system(dxdt=sysd["equations"], states={{s: 0.0 for s in sysd["states"]}},
                            parameters={{p: 0.0 for p in sysd["parameters"]}}, constants=sysd["constants"],
-                           precision=prec, name="fixture_" + name, strict=True)
+                           drivers=sysd.get("drivers"), precision=prec, name="fixture_" + name, strict=True)
 inits, params = case_inputs(case)
 solver = Solver(system, algorithm=case["algorithm"], cache=False, auto_memory=False, **case["kwargs"])
 t = time.time()
-res = solver.solve(inits.astype(prec), params.astype(prec), duration=case["duration"],
+res = solver.solve(inits.astype(prec), params.astype(prec), drivers=drivers, duration=case["duration"],
                    grid_type="verbatim", nan_error_trajectories=False)
 elapsed = time.time() - t
 out = dict(inits=inits, params=params, status=np.asarray(res.status_codes), elapsed=elapsed)
@@ -54,6 +55,13 @@ if res.iteration_counters is not None:
 if res.state_summaries is not None:
     out["state_summaries"] = np.asarray(res.state_summaries)
 out["summaries_legend"] = np.array(json.dumps({{str(k): v for k, v in res.summaries_legend.items()}}))
+if drivers is not None:
+    from cubie.array_interpolator import ArrayInterpolator
+    interp = ArrayInterpolator(prec, dict(drivers))
+    out["driver_coefficients"] = np.asarray(interp.coefficients)
+    out["driver_meta"] = np.array([interp.driver_sample_period, interp.t0, interp.num_segments,
+                                   float(interp.wrap), float(interp.boundary_condition == "clamped"),
+                                   float(interp.order)])
 np.savez_compressed({outfile!r}, **out)
 print(name, "ok", round(elapsed, 2), "s; status", out["status"].tolist())
 """

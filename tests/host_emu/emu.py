@@ -83,11 +83,17 @@ def compile_emulated(source: str):
 
 
 def run_emulated(solver, inits, params, duration, settling_time=0.0, t0=0.0, kernel="plain",
-                 durations=None, tol_scale=None):
+                 durations=None, tol_scale=None, drivers=None):
     """Integrate with the solver's generated kernel on the CPU; returns a dict
     of output arrays laid out like ``SolveResult``."""
     from cubie_b200 import _native
-    prep = solver.prepare(duration, settling_time, t0, None, durations, load=False)
+    interp = None
+    coeffs = None
+    if drivers is not None:
+        from cubie_b200.interpolator import ArrayInterpolator
+        interp = ArrayInterpolator.from_system(solver.system, drivers, solver.precision)
+        coeffs = np.ascontiguousarray(interp.coefficients, dtype=solver.precision)
+    prep = solver.prepare(duration, settling_time, t0, interp, durations, load=False)
     spec = prep["spec"]
     gk = prep["gen"]
     lib = compile_emulated(gk.source)
@@ -131,7 +137,8 @@ def run_emulated(solver, inits, params, duration, settling_time=0.0, t0=0.0, ker
     # make_args zeroes the work counter through .zero_(); emulate that
     bufs["work"][:] = 0
     wb["work"].zero_ = lambda: None
-    args = solver.make_args(prep, wb, _P(inits), _P(params), None, n_runs, duration, settling_time, t0,
+    args = solver.make_args(prep, wb, _P(inits), _P(params), _P(coeffs) if coeffs is not None else None, n_runs,
+                            duration, settling_time, t0,
                             _P(dur) if dur is not None else None, _P(tsc) if tsc is not None else None)
     block = 32
     grid = (n_runs + block - 1) // block

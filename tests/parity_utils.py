@@ -2,7 +2,11 @@
 
 import numpy as np
 
-from cases import CASES, case_inputs
+from pathlib import Path
+
+from cases import CASES, case_drivers, case_inputs
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
 
 
 def build_case_system(case):
@@ -11,13 +15,27 @@ def build_case_system(case):
     prec = np.dtype(case["precision"]).type
     return create_ODE_system(sd["equations"], states={s: 0.0 for s in sd["states"]},
                              parameters={p: 0.0 for p in sd["parameters"]}, constants=sd["constants"],
-                             precision=prec, strict=True)
+                             drivers=sd.get("drivers"), precision=prec, strict=True)
+
+
+def oracle_driver_table(case, name):
+    """The reference's own coefficient table for a driven case (stored in
+    its fixture), as an oracle driver evaluator."""
+    from oracle import DriverTable
+    ref = np.load(GOLDEN / f"ref_{name}.npz")
+    period, t0, _, wrap, padded, _ = ref["driver_meta"]
+    return DriverTable(ref["driver_coefficients"], period, t0, bool(wrap), bool(padded),
+                       np.dtype(case["precision"]).type)
 
 
 def run_oracle(case, **overrides):
     from oracle import OracleSystem, integrate
     sd = case["system"]
-    osys = OracleSystem(sd["equations"], sd["states"], sd["parameters"], sd["constants"])
+    osys = OracleSystem(sd["equations"], sd["states"], sd["parameters"], sd["constants"],
+                        drivers=sd.get("drivers", ()))
+    if sd.get("drivers"):
+        name = next(n for n, c in CASES.items() if c is case)
+        osys.driver_table = oracle_driver_table(case, name)
     inits, params = case_inputs(case)
     kw = dict(case["kwargs"])
     kw["precision"] = np.dtype(case["precision"]).type

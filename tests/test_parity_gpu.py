@@ -13,7 +13,7 @@ from pathlib import Path
 import numpy as np
 import pytest
 
-from cases import CASES, case_inputs
+from cases import CASES, case_drivers, case_inputs
 from parity_utils import build_case_system, run_oracle, tol_units
 
 GOLDEN = Path(__file__).resolve().parent / "golden"
@@ -28,8 +28,8 @@ def _solve(case, kernel="plain", **extra):
     kw.update(extra)
     solver = Solver(system, algorithm=case["algorithm"], kernel=kernel, **kw)
     prec = np.dtype(case["precision"]).type
-    return solver.solve(inits.astype(prec), params.astype(prec), duration=case["duration"],
-                        nan_error_trajectories=False)
+    return solver.solve(inits.astype(prec), params.astype(prec), drivers=case_drivers(case),
+                        duration=case["duration"], nan_error_trajectories=False)
 
 
 def _bars(name):
