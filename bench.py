@@ -178,6 +178,66 @@ def measured_peaks():
 
 FHN = ["dV = V - V**3 / 3 - w + I", "dw = (V + a - b * w) / tau"]
 ADJ_T = 200.0
+LORENZ = ["dx = sigma * (y - x)", "dy = x * (rho - z) - y", "dz = x * y - beta * z"]
+
+
+def lorenz_arm(args, dev):
+    """Lorenz ensemble (sigma 10, beta 8/3 constants; rho ~ U[20,35],
+    x0 ~ U[-10,10]^3; seed 1): DP54, PI controller defaults, rtol 1e-6,
+    atol 1e-8, t in [0, 10], every state saved every 0.01 (1001 rows incl.
+    t0) plus mean and max over each 10-unit window sampled every 0.01, FP32
+    with FP64 time and control, persistent launch.  Solved = status 0 and
+    the final state within 10 tolerance units of an FP64 solve at 1e-12 on
+    256 of the runs (Lorenz is chaotic, so the comparison is the final state
+    only)."""
+    import torch
+    from cubie_b200 import Solver, create_ODE_system, _native
+    n = args.lorenz_n
+    rng = np.random.default_rng(1)
+    rho = rng.uniform(20.0, 35.0, n)
+    x0 = rng.uniform(-10.0, 10.0, (3, n))
+    out = {}
+    kw = dict(algorithm="dormand-prince-54", rtol=1e-6, atol=1e-8, save_every=0.01, summarise_every=10.0,
+              sample_summaries_every=0.01, output_types=["state", "mean", "max"], device=dev.index)
+    sys32 = create_ODE_system(LORENZ, states={"x": 1.0, "y": 0.0, "z": 0.0}, parameters={"rho": 21.0},
+                              constants={"sigma": 10.0, "beta": 8.0 / 3.0}, precision=np.float32)
+    sys64 = create_ODE_system(LORENZ, states={"x": 1.0, "y": 0.0, "z": 0.0}, parameters={"rho": 21.0},
+                              constants={"sigma": 10.0, "beta": 8.0 / 3.0}, precision=np.float64)
+    solver = Solver(sys32, mixed_precision=True, **kw)
+    truth = Solver(sys64, **dict(kw, rtol=1e-12, atol=1e-12, output_types=["state"]))
+    T = min(256, n)
+    tr = truth.solve(x0[:, :T], rho[None, :T], duration=10.0, nan_error_trajectories=False)
+    y_true = tr.state[100].astype(np.float64)
+    prep = solver.prepare(10.0)
+    inits = torch.as_tensor(x0, device=dev).float().contiguous()
+    params = torch.as_tensor(rho[None, :], device=dev).float().contiguous()
+    bufs = solver.allocate_outputs(prep, n, dev, torch.float32)
+    stream = torch.cuda.current_stream(dev)
+    flush = torch.empty(int(256e6) // 4, dtype=torch.int32, device=dev)
+    times = []
+    for it in range(args.warmup + args.steps):
+        a = solver.make_args(prep, bufs, inits, params, None, n, 10.0, 0.0, 0.0)
+        _native.flush_l2(flush.data_ptr(), flush.numel() * 4, stream.cuda_stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        prep["module"].launch(a, 1, solver.block_size, 0, stream.cuda_stream)
+        e1.record(stream)
+        e1.synchronize()
+        if it >= args.warmup:
+            times.append(e0.elapsed_time(e1))
+    y = bufs["state"][100][:, :T].double().cpu().numpy()
+    st = bufs["status"].cpu().numpy()
+    err = np.max(np.abs(y - y_true) / (1e-8 + 1e-6 * np.abs(y_true)), axis=0)
+    frac = float(np.mean((st[:T] == 0) & (err <= SOLVED_TOL_UNITS)))
+    ms = float(np.mean(times))
+    out_bytes = bufs["state"].numel() * 4 + bufs["state_sum"].numel() * 4
+    del flush
+    return {"workload": "Lorenz, rho~U[20,35], x0~U[-10,10]^3, DP54 rtol 1e-6 atol 1e-8, t in [0,10], 1001 saved "
+                        "rows of 3 states, mean+max summaries, FP32 + FP64 control, persistent launch",
+            "n_systems": n, "ms": ms, "value": n * frac / (ms * 1e-3), "unit": "systems/s",
+            "solved_fraction": frac, "output_bytes": int(out_bytes),
+            "output_gbs": out_bytes / (ms * 1e-3) / 1e9}
+
 
 
 def adjoint_arm(args, dev):
@@ -413,6 +473,8 @@ def gpu_arm(args, rank: int, world: int, dist):
         peak_fp32 = _native.fp32_peak(dev.index) / 1e12
         hbm_bytes = (x0.size * 4 + mu.size * 4 + durs.size * 8 + 2 * 2 * n * 4 + n * 4)
         peaks = measured_peaks()
+        lor = lorenz_arm(args, dev) if args.lorenz_n > 0 else None
+        log('lorenz', lor)
         adj = adjoint_arm(args, dev) if args.adj_n > 0 else None
         log('adjoint', adj)
         cpu = cpu_reference(per_core=args.cpu_per_core, max_steps=args.cpu_max_steps) if not args.no_cpu else None
@@ -463,6 +525,7 @@ def gpu_arm(args, rank: int, world: int, dist):
                                     "config": "plain one-thread-per-run launch, same algorithm and precision "
                                               "settings as the headline line"},
             "adjoint": adj,
+            "lorenz": lor,
             "cpu_baseline": cpu,
             "clocks": clocks.summary(),
         }
@@ -501,6 +564,7 @@ def main():
     ap.add_argument("--cpu-max-steps", type=int, default=3000)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--adj-n", type=int, default=262144, help="FitzHugh-Nagumo adjoint leg size (0: skip)")
+    ap.add_argument("--lorenz-n", type=int, default=4096, help="Lorenz saved-trajectory leg size (0: skip)")
     ap.add_argument("--adj-steps", type=int, default=3)
     ap.add_argument("--adj-warmup", type=int, default=1)
     args = ap.parse_args()
