@@ -11,11 +11,15 @@ from .symbolic import SymbolicODE, create_ODE_system
 from .solver import Solver, solve_ivp
 from .solveresult import SolveResult, SolveSpec
 from .tableaus import TABLEAU_REGISTRY, Tableau, resolve_algorithm
+from .graph import GraphSolve
+from .interpolator import ArrayInterpolator
+from .adjoint import AdjointIntegrator, solve_ivp_adjoint
+from .autotune import autotune
 
 __version__ = "0.1.0"
 
 __all__ = [
     "CUBIE_RESULT_CODES", "decode_status_codes", "SymbolicODE", "create_ODE_system",
     "Solver", "solve_ivp", "SolveResult", "SolveSpec", "TABLEAU_REGISTRY", "Tableau",
-    "resolve_algorithm",
+    "resolve_algorithm", "GraphSolve", "ArrayInterpolator", "AdjointIntegrator", "solve_ivp_adjoint", "autotune",
 ]

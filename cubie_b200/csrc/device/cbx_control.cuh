@@ -43,7 +43,7 @@ struct Controller {
 #pragma unroll
         for (int i = 0; i < N; ++i) {
             const C e = pymax(C(absv(err[i])), C(1e-16));
-            const C tol = C(cbx_atol[i]) + C(cbx_rtol[i]) * tol_scale * pymax(C(absv(ynew[i])), C(absv(y[i])));
+            const C tol = C(Cfg::atol(i)) + C(Cfg::rtol(i)) * tol_scale * pymax(C(absv(ynew[i])), C(absv(y[i])));
             const C ratio = e / tol;
             nrm2 += ratio * ratio;
         }

@@ -13,7 +13,7 @@ template <class Cfg>
 __device__ __forceinline__ typename Cfg::C krylov_tol(int i, typename Cfg::R ref, typename Cfg::C scale) {
     using C = typename Cfg::C;
     const int k = i % Cfg::N;
-    C t = C(cbx_katol[k]) + C(cbx_krtol[k]) * scale * C(absv(ref));
+    C t = C(Cfg::katol(k)) + C(Cfg::krtol(k)) * scale * C(absv(ref));
     return pymax(t, C(1e-16));
 }
 

@@ -359,7 +359,7 @@ struct FirkProblem {
 #pragma unroll
             for (int k = 0; k < N; ++k) {
                 const R ref = pymax(absv(Y[k]), absv(base[k]));
-                C tol = C(cbx_natol[k]) + C(cbx_nrtol[k]) * ctx->tol_scale * C(ref);
+                C tol = C(Cfg::natol(k)) + C(Cfg::nrtol(k)) * ctx->tol_scale * C(ref);
                 tol = pymax(tol, C(1e-16));
                 const C ratio = C(delta[i * N + k]) / tol;
                 nrm2 += ratio * ratio;
@@ -539,7 +539,7 @@ struct DirkProblem {
         for (int k = 0; k < N; ++k) {
             const R sv = base[k] + a * z[k];
             const R ref = pymax(absv(sv), absv(step_start[k]));
-            C tol = C(cbx_natol[k]) + C(cbx_nrtol[k]) * ctx->tol_scale * C(ref);
+            C tol = C(Cfg::natol(k)) + C(Cfg::nrtol(k)) * ctx->tol_scale * C(ref);
             tol = pymax(tol, C(1e-16));
             const C ratio = C(delta[k]) / tol;
             nrm2 += ratio * ratio;

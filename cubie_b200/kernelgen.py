@@ -200,9 +200,14 @@ class GeneratedKernel:
         return hashlib.sha256(self.source.encode()).hexdigest()[:24]
 
 
-def generate_kernel(system: SymbolicODE, spec: KernelSpec, gen: Optional[GeneratedSystem] = None) -> GeneratedKernel:
-    """Return the complete CUDA translation unit for ``spec``."""
-    gen = gen or generate_system(system, second_order=spec.adjoint and spec.tableau.kind == ROSENBROCK)
+DEVICE_INCLUDES = ['#include "cbx_common.cuh"', '#include "cbx_args.h"', '#include "cbx_steps.cuh"',
+                   '#include "cbx_control.cuh"', '#include "cbx_loop.cuh"']
+
+
+def family_block(system: SymbolicODE, spec: KernelSpec, gen: GeneratedSystem, ns: str) -> List[str]:
+    """The generated pieces of one configuration (system struct, tolerance
+    tables, index tables, tableau, summary metrics and ``Cfg``), to be
+    placed inside namespace ``ns``."""
     tab = spec.tableau
     n = system.num_states
     rtype = "float" if np.dtype(spec.precision) == np.float32 else "double"
@@ -237,17 +242,11 @@ def generate_kernel(system: SymbolicODE, spec: KernelSpec, gen: Optional[Generat
             return float(np.float32(v))
         return float(v)
 
-    lines: List[str] = []
-    lines.append("// generated by cubie_b200.kernelgen; do not edit")
-    lines.append('#include "cbx_common.cuh"')
-    lines.append('#include "cbx_args.h"')
-    lines.append(gen.source)
-    lines.append(_const_array("cbx_atol", ctype, [castp(v) for v in np.broadcast_to(spec.atol, (n,))]))
-    lines.append(_const_array("cbx_rtol", ctype, [castp(v) for v in np.broadcast_to(spec.rtol, (n,))]))
-    lines.append(_const_array("cbx_katol", ctype, [castp(v) for v in np.broadcast_to(katol, (n,))]))
-    lines.append(_const_array("cbx_krtol", ctype, [castp(v) for v in np.broadcast_to(krtol, (n,))]))
-    lines.append(_const_array("cbx_natol", ctype, [castp(v) for v in np.broadcast_to(natol, (n,))]))
-    lines.append(_const_array("cbx_nrtol", ctype, [castp(v) for v in np.broadcast_to(nrtol, (n,))]))
+    lines: List[str] = [gen.source]
+    tol_arrays = [("atol", spec.atol), ("rtol", spec.rtol), ("katol", katol), ("krtol", krtol), ("natol", natol),
+                  ("nrtol", nrtol)]
+    for name, vals in tol_arrays:
+        lines.append(_const_array(f"cbx_{name}", ctype, [castp(v) for v in np.broadcast_to(vals, (n,))]))
     idx_fns = []
     for fname, vals in (("saved_state", spec.saved_state_indices), ("saved_obs", spec.saved_observable_indices),
                         ("summ_state", spec.summarised_state_indices), ("summ_obs", spec.summarised_observable_indices)):
@@ -255,20 +254,18 @@ def generate_kernel(system: SymbolicODE, spec: KernelSpec, gen: Optional[Generat
         idx_fns.append(f"    static __host__ __device__ constexpr int {fname}(int k) {{ constexpr int v[{len(vv)}] = "
                        f"{{{', '.join(str(v) for v in vv)}}}; return v[k]; }}")
     lines.append("struct Idx {\n" + "\n".join(idx_fns) + "\n};")
-    lines.append('#include "cbx_steps.cuh"')
-    lines.append('#include "cbx_control.cuh"')
     lines.append(tableau_struct(tab, spec.precision, dense))
     lines.append(summ.device_struct())
     save_every = castp(spec.save_every) if spec.save_every is not None else 0.0
     sample_every = castp(spec.sample_summaries_every) if spec.sample_summaries_every is not None else 0.0
     cfg = [
         "struct Cfg {",
-        "    using Sys = System;",
+        f"    using Sys = {ns}::System;",
         f"    using R = {rtype};",
         f"    using C = {ctype};",
-        "    using Tab = ::Tab;",
-        "    using Summ = ::Summ;",
-        "    using Idx = ::Idx;",
+        f"    using Tab = {ns}::Tab;",
+        f"    using Summ = {ns}::Summ;",
+        f"    using Idx = {ns}::Idx;",
         f"    static constexpr int N = Sys::N, NP = Sys::NP, ND = Sys::ND, NO = Sys::NO, S = Tab::S;",
         f"    static constexpr int ALGO = {ALGO_IDS[tab.kind]};",
         f"    static constexpr int CTRL = {CTRL_IDS[ctl]};",
@@ -318,13 +315,29 @@ def generate_kernel(system: SymbolicODE, spec: KernelSpec, gen: Optional[Generat
         f"    static constexpr int BLOCK = {int(spec.block_size)};",
         f"    static constexpr int MIN_BLOCKS = {max(int(spec.min_blocks_per_sm), 1)};",
         f"    using Step = {STEP_TYPES[tab.kind]};",
+        *[f"    static __device__ __forceinline__ C {name}(int i) {{ return cbx_{name}[i]; }}" for name, _ in tol_arrays],
         "};",
     ]
     lines.append("\n".join(cfg))
+    return lines
+
+
+def generate_kernel(system: SymbolicODE, spec: KernelSpec, gen: Optional[GeneratedSystem] = None) -> GeneratedKernel:
+    """Return the complete CUDA translation unit for ``spec``: the device
+    headers, then the configuration's generated pieces in namespace
+    ``cbxsys``, then the kernels instantiated for ``cbxsys::Cfg``."""
+    gen = gen or generate_system(system, second_order=spec.adjoint and spec.tableau.kind == ROSENBROCK)
+    tab = spec.tableau
+    lines = ["// generated by cubie_b200.kernelgen; do not edit"]
     if int(spec.min_blocks_per_sm) > 1:
         lines.append("#define CBX_LAUNCH_BOUNDS(CFG) __launch_bounds__(CFG::BLOCK, CFG::MIN_BLOCKS)")
-    lines.append('#include "cbx_loop.cuh"')
-    lines.append("CBX_DEFINE_KERNELS(Cfg)")
+    lines += DEVICE_INCLUDES
+    if spec.adjoint:
+        lines.append('#include "cbx_adjoint.cuh"')
+    lines.append("namespace cbxsys {")
+    lines += family_block(system, spec, gen, "cbxsys")
+    lines.append("}  // namespace cbxsys")
+    lines.append("CBX_DEFINE_KERNELS(cbxsys::Cfg)")
     if spec.adjoint:
         if tab.kind not in ADJOINT_FAMILIES:
             raise NotImplementedError(f"no discrete adjoint for the {tab.kind} family "
@@ -332,6 +345,5 @@ def generate_kernel(system: SymbolicODE, spec: KernelSpec, gen: Optional[Generat
         if tab.kind == ROSENBROCK and (system.num_drivers > 0 or any(
                 TIME in e.free_symbols for e in system.rhs_expressions())):
             raise NotImplementedError("the Rosenbrock adjoint needs an autonomous system without drivers")
-        lines.append('#include "cbx_adjoint.cuh"')
-        lines.append("CBX_DEFINE_ADJOINT_KERNELS(Cfg)")
+        lines.append("CBX_DEFINE_ADJOINT_KERNELS(cbxsys::Cfg)")
     return GeneratedKernel(source="\n".join(lines) + "\n", system=gen, spec=spec)

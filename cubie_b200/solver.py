@@ -132,7 +132,9 @@ class Solver:
         self.kernel_kind = execution.get("kernel", "persistent")
         if self.kernel_kind not in ("plain", "persistent"):
             raise ValueError("kernel must be 'plain' or 'persistent'")
-        self.block_size = int(execution.get("block_size", 128))
+        bs = execution.get("block_size", 128)
+        self.autotune_pending = isinstance(bs, str) and bs == "auto"
+        self.block_size = 128 if self.autotune_pending else int(bs)
         self.min_blocks_per_sm = int(execution.get("min_blocks_per_sm", 1))
         self.adjoint = bool(execution.get("adjoint", False))
         self.max_steps = int(execution.get("max_steps", 0))
@@ -509,6 +511,13 @@ class Solver:
         torch = _torch()
         if not torch.cuda.is_available():
             raise RuntimeError("cubie_b200 needs a CUDA device: no GPU is visible")
+        if self.autotune_pending:
+            from .autotune import autotune
+            tuned = autotune(self, inits, params, duration, durations=durations)
+            self.block_size, self.min_blocks_per_sm = int(tuned["block"]), int(tuned["min_blocks"])
+            self.autotune_result = tuned
+            self.autotune_pending = False
+            self.__dict__["_prepared"] = {}
         prep = self.prepare(duration, settling_time, t0, interp, durations)
         spec: KernelSpec = prep["spec"]
         dev = torch.device("cuda", self.device)
@@ -549,6 +558,12 @@ class Solver:
         e1.synchronize()
         self.last_kernel_ms = e0.elapsed_time(e1)
         return self.collect(prep, bufs, n_runs, duration, settling_time, t0, nan_error_trajectories, on_device)
+
+    def graph(self, n_runs: int, duration: float, **kwargs):
+        """A :class:`~cubie_b200.graph.GraphSolve`: this solve captured as
+        one CUDA graph (transfers, launch, read-back) for repeated calls."""
+        from .graph import GraphSolve
+        return GraphSolve(self, n_runs, duration, **kwargs)
 
     def allocate_outputs(self, prep, n_runs: int, dev, tdtype) -> Dict[str, Any]:
         torch = _torch()

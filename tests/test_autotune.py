@@ -1,0 +1,56 @@
+"""Launch-shape autotuner: selection, caching and configuration identity
+(CPU, with an injected timer)."""
+
+import numpy as np
+import pytest
+
+VDP = ["dx = y", "dy = mu * (1 - x**2) * y - x"]
+
+
+def _solver(**kw):
+    from cubie_b200 import Solver, create_ODE_system
+    sysm = create_ODE_system(VDP, states={"x": 2.0, "y": 0.0}, parameters={"mu": 10.0}, precision=np.float32)
+    return Solver(sysm, algorithm="ros3p", output_types=["state"], **kw)
+
+
+def test_choose_picks_fastest_and_skips_failures():
+    from cubie_b200.autotune import choose
+    assert choose({(128, 1): 5.0, (64, 1): 3.0, (256, 1): float("nan")}) == (64, 1)
+    assert choose({(128, 1): 2.0, (64, 1): 2.0}) == (128, 1)
+    with pytest.raises(RuntimeError):
+        choose({(128, 1): float("nan")})
+
+
+def test_autotune_uses_timer_and_caches(tmp_path, monkeypatch):
+    from cubie_b200.autotune import autotune
+    monkeypatch.setenv("CUBIE_B200_CACHE_DIR", str(tmp_path))
+    solver = _solver()
+    calls = []
+
+    def fake(v):
+        calls.append((v.block_size, v.min_blocks_per_sm))
+        return {(128, 1): 9.0, (64, 1): 7.5, (256, 1): 8.0, (128, 6): 7.0}[(v.block_size, v.min_blocks_per_sm)]
+
+    cands = [(128, 1), (64, 1), (256, 1), (128, 6)]
+    r = autotune(solver, None, None, 2.0, candidates=cands, timer=fake)
+    assert (r["block"], r["min_blocks"], r["cached"]) == (128, 6, False)
+    assert calls == cands
+    r2 = autotune(solver, None, None, 2.0, candidates=cands, timer=fake)
+    assert r2["cached"] and (r2["block"], r2["min_blocks"]) == (128, 6)
+    assert len(calls) == len(cands)          # served from the cache
+    # a different configuration is tuned separately
+    other = _solver(rtol=1e-4)
+    autotune(other, None, None, 2.0, candidates=cands, timer=fake)
+    assert len(calls) == 2 * len(cands)
+
+
+def test_config_key_ignores_launch_shape():
+    from cubie_b200.autotune import config_key, variant
+    s = _solver()
+    assert config_key(s, 2.0, "gpu") == config_key(variant(s, 256, 3), 2.0, "gpu")
+    assert config_key(s, 2.0, "gpu") != config_key(s, 2.0, "other-gpu")
+
+
+def test_block_size_auto_is_pending_until_first_solve():
+    s = _solver(block_size="auto")
+    assert s.autotune_pending and s.block_size == 128
