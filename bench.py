@@ -321,6 +321,106 @@ def adjoint_arm(args, dev):
             "checkpoint_and_record_bytes": list(integ.sizes(prep))}
 
 
+ROBERTSON = ["dy1 = -k1 * y1 + k3 * y2 * y3", "dy2 = k1 * y1 - k3 * y2 * y3 - k2 * y2**2", "dy3 = k2 * y2**2"]
+
+
+def hetero_arm(args, dev):
+    """2^20 runs split evenly by system: Lorenz (rho~U[20,35], x0~U[-10,10]^3;
+    DP54), stiff Van der Pol (mu=10^U[0,3], x0~U[-2,2]^2; ROS3P + GMRES) and
+    Robertson (k1=0.04, k2=3e7, k3=1e4 each x U[0.5,2], y0=(1,0,0); ROS3P +
+    GMRES); per-run rtol = 10^U[-8,-4] (a per-run scale on rtol 1e-4),
+    per-run horizon 10^U[0,3]; FP32 stepping with FP64 time, control and
+    norms; final state only; one heterogeneous persistent launch replayed as
+    a CUDA graph.  Solved: status 0, and for Van der Pol and Robertson the
+    final state within 10 tolerance units (of that run's rtol) of an FP64
+    Radau solve at rtol 1e-11 on 512 runs per system; Lorenz runs are
+    checked by status only (the final state of a chaotic run over hundreds
+    of time units has no tolerance-scale reference)."""
+    import torch
+    from cubie_b200 import Solver, create_ODE_system, _native
+    from cubie_b200.hetero import HeteroSolver
+    n_total = args.c5_n
+    n = n_total // 3
+    rng = np.random.default_rng(5)
+    f32 = np.float32
+    lor = create_ODE_system(LORENZ, states={"x": 1.0, "y": 0.0, "z": 0.0}, parameters={"rho": 21.0},
+                            constants={"sigma": 10.0, "beta": 8.0 / 3.0}, precision=f32)
+    vdp = create_ODE_system(VDP, states={"x": 2.0, "y": 0.0}, parameters={"mu": 10.0}, precision=f32)
+    rob = create_ODE_system(ROBERTSON, states={"y1": 1.0, "y2": 0.0, "y3": 0.0},
+                            parameters={"k1": 0.04, "k2": 3e7, "k3": 1e4}, precision=f32)
+    common = dict(rtol=1e-4, output_types=["state"], mixed_precision=True, device=dev.index)
+    gm = dict(linear_correction_type="gmres", preconditioner_type=None)
+    solvers = [Solver(lor, algorithm="dormand-prince-54", atol=1e-8, **common),
+               Solver(vdp, algorithm="ros3p", atol=1e-8, **gm, **common),
+               Solver(rob, algorithm="ros3p", atol=1e-10, **gm, **common)]
+    batches = []
+    inputs = [(rng.uniform(-10, 10, (3, n)), rng.uniform(20, 35, (1, n))),
+              (rng.uniform(-2, 2, (2, n)), (10.0 ** rng.uniform(0, 3, n))[None, :]),
+              (np.tile([[1.0], [0.0], [0.0]], (1, n)),
+               np.stack([0.04 * rng.uniform(0.5, 2, n), 3e7 * rng.uniform(0.5, 2, n), 1e4 * rng.uniform(0.5, 2, n)]))]
+    for x0, p in inputs:
+        rtol = 10.0 ** rng.uniform(-8, -4, n)
+        horizon = 10.0 ** rng.uniform(0, 3, n)
+        batches.append(dict(initial_values=torch.as_tensor(x0, device=dev).float(),
+                            parameters=torch.as_tensor(p, device=dev).float(),
+                            duration=float(horizon.max()), durations=horizon, tol_scale=rtol / 1e-4,
+                            _rtol=rtol, _x0=x0, _p=p))
+    hs = HeteroSolver(solvers)
+    run = hs.setup(batches)
+    graph = run.graph()
+    stream = torch.cuda.current_stream(dev)
+    flush = torch.empty(int(256e6) // 4, dtype=torch.int32, device=dev)
+    times = []
+    for it in range(1 + args.c5_steps):
+        _native.flush_l2(flush.data_ptr(), flush.numel() * 4, stream.cuda_stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        graph.replay()
+        e1.record(stream)
+        e1.synchronize()
+        if it >= 1:
+            times.append(e0.elapsed_time(e1))
+    del graph
+    hs.last_kernel_ms = float(np.mean(times))
+    results = run.collect(nan_error_trajectories=False)
+    fam = {}
+    solved_total = 0.0
+    for name, s64sys, b, r in (("lorenz", None, batches[0], results[0]),
+                               ("vdp", VDP, batches[1], results[1]), ("robertson", ROBERTSON, batches[2], results[2])):
+        ok = r.status_codes == 0
+        frac = float(np.mean(ok))
+        if s64sys is not None:
+            T = 512
+            states = {"x": 2.0, "y": 0.0} if name == "vdp" else {"y1": 1.0, "y2": 0.0, "y3": 0.0}
+            params = {"mu": 10.0} if name == "vdp" else {"k1": 0.04, "k2": 3e7, "k3": 1e4}
+            sys64 = create_ODE_system(s64sys, states=states, parameters=params, precision=np.float64)
+            truth = Solver(sys64, algorithm="radau", rtol=1e-11, atol=1e-13, dt_min=1e-14, output_types=["state"],
+                           linear_correction_type="gmres", preconditioner_type=None, max_steps=20_000_000,
+                           device=dev.index)
+            tr = truth.solve(b["_x0"][:, :T], b["_p"][:, :T], duration=b["duration"], durations=b["durations"][:T],
+                             nan_error_trajectories=False)
+            y = r.state[-1][:, :T].astype(np.float64)
+            yt = tr.state[-1].astype(np.float64)
+            atol = solvers[1 if name == "vdp" else 2].atol
+            atol = float(np.max(atol)) if np.ndim(atol) else float(atol)
+            err = np.max(np.abs(y - yt) / (atol + b["_rtol"][None, :T] * np.abs(yt)), axis=0)
+            good = (tr.status_codes == 0)
+            frac = float(np.sum(ok[:T] & good & (err <= SOLVED_TOL_UNITS)) / max(1, np.sum(good)))
+            fam[name] = {"solved_fraction": frac, "status_ok_fraction": float(np.mean(ok)),
+                         "error_tol_units_pct50_90_99": [float(np.percentile(err[good], q)) for q in (50, 90, 99)],
+                         "totals": r.totals}
+        else:
+            fam[name] = {"solved_fraction": frac, "status_ok_fraction": frac, "totals": r.totals}
+        solved_total += n * fam[name]["solved_fraction"]
+    ms = float(np.mean(times))
+    del flush
+    return {"workload": "2^20 runs split evenly: Lorenz DP54, stiff VdP ROS3P+GMRES, Robertson ROS3P+GMRES; per-run "
+                        "rtol 10^U[-8,-4], per-run horizon 10^U[0,3]; FP32 stepping + FP64 control; one "
+                        "heterogeneous persistent launch replayed as a CUDA graph",
+            "n_systems": 3 * n, "ms": ms, "value": solved_total / (ms * 1e-3), "unit": "systems/s",
+            "families": fam, "graph": True}
+
+
 def plain_wave(sysm, device: int) -> int:
     """Runs in one full resident wave of the plain kernel on this GPU."""
     from cubie_b200 import Solver, _native
@@ -475,6 +575,8 @@ def gpu_arm(args, rank: int, world: int, dist):
         peaks = measured_peaks()
         lor = lorenz_arm(args, dev) if args.lorenz_n > 0 else None
         log('lorenz', lor)
+        c5 = hetero_arm(args, dev) if args.c5_n > 0 else None
+        log('hetero', c5)
         adj = adjoint_arm(args, dev) if args.adj_n > 0 else None
         log('adjoint', adj)
         cpu = cpu_reference(per_core=args.cpu_per_core, max_steps=args.cpu_max_steps) if not args.no_cpu else None
@@ -526,6 +628,7 @@ def gpu_arm(args, rank: int, world: int, dist):
                                               "settings as the headline line"},
             "adjoint": adj,
             "lorenz": lor,
+            "heterogeneous": c5,
             "cpu_baseline": cpu,
             "clocks": clocks.summary(),
         }
@@ -565,6 +668,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--adj-n", type=int, default=262144, help="FitzHugh-Nagumo adjoint leg size (0: skip)")
     ap.add_argument("--lorenz-n", type=int, default=4096, help="Lorenz saved-trajectory leg size (0: skip)")
+    ap.add_argument("--c5-n", type=int, default=1 << 20, help="heterogeneous three-system leg size (0: skip)")
+    ap.add_argument("--c5-steps", type=int, default=2)
     ap.add_argument("--adj-steps", type=int, default=3)
     ap.add_argument("--adj-warmup", type=int, default=1)
     args = ap.parse_args()

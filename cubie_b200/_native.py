@@ -75,11 +75,24 @@ class AdjointArgs(ctypes.Structure):
     ]
 
 
+class HeteroArgs(ctypes.Structure):
+    """Mirror of ``cbx_hetero_args`` (cubie_b200/csrc/device/cbx_args.h)."""
+
+    MAX_FAMILIES = 8
+    _fields_ = [
+        ("family", SolveArgs * 8),
+        ("first_run", ctypes.c_longlong * 9),
+        ("work_counter", ctypes.c_void_p),
+        ("n_families", ctypes.c_int),
+        ("reserved", ctypes.c_int),
+    ]
+
+
 EXPORTED = (
     "cbx_version", "cbx_last_error", "cbx_nvrtc_version", "cbx_compile", "cbx_free",
     "cbx_module_load", "cbx_module_create", "cbx_module_destroy", "cbx_kernel_info",
     "cbx_occupancy", "cbx_solve", "cbx_device_info", "cbx_fp32_peak_probe", "cbx_flush_l2",
-    "cbx_solve_noalloc", "cbx_adjoint_info", "cbx_adjoint_launch",
+    "cbx_solve_noalloc", "cbx_adjoint_info", "cbx_adjoint_launch", "cbx_solve_hetero",
 )
 
 _lib = None
@@ -134,6 +147,8 @@ def lib():
         L.cbx_flush_l2.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]
         L.cbx_solve_noalloc.argtypes = [ctypes.c_void_p, ctypes.POINTER(SolveArgs), ctypes.c_int, ctypes.c_int,
                                         ctypes.c_void_p]
+        L.cbx_solve_hetero.argtypes = [ctypes.c_void_p, ctypes.POINTER(HeteroArgs), ctypes.c_int, ctypes.c_int,
+                                       ctypes.c_void_p]
         L.cbx_adjoint_info.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong),
                                        ctypes.POINTER(ctypes.c_longlong)]
         L.cbx_adjoint_launch.argtypes = [ctypes.c_void_p, ctypes.POINTER(SolveArgs), ctypes.POINTER(AdjointArgs),
@@ -233,6 +248,10 @@ class Module:
     def launch(self, args: SolveArgs, kernel: int, block: int, grid: int = 0, stream: int = 0) -> None:
         _check(lib().cbx_solve(self._handle, ctypes.byref(args), kernel, block, grid, ctypes.c_void_p(stream)),
                "cbx_solve")
+
+    def launch_hetero(self, args: "HeteroArgs", block: int, grid: int = 0, stream: int = 0) -> None:
+        _check(lib().cbx_solve_hetero(self._handle, ctypes.byref(args), block, grid, ctypes.c_void_p(stream)),
+               "cbx_solve_hetero")
 
     def adjoint_sizes(self) -> tuple:
         """(bytes of one checkpoint image, bytes of one replay record)."""

@@ -73,4 +73,20 @@ typedef struct cbx_adjoint_args {
     int max_ckpts;
 } cbx_adjoint_args;
 
+/* Several configurations ("families") in one persistent launch.  Global
+ * run r belongs to family k when first_run[k] <= r < first_run[k + 1] and is
+ * run r - first_run[k] of family[k] (that family's own inputs, outputs,
+ * status words and, when non-NULL, iteration totals).  The families'
+ * work_counter fields are unused: ``work_counter`` points at
+ * CBX_MAX_FAMILIES zeroed 64-bit counters, one per family.
+ * first_run[n_families] is the total number of runs. */
+#define CBX_MAX_FAMILIES 8
+typedef struct cbx_hetero_args {
+    cbx_solve_args family[CBX_MAX_FAMILIES];
+    long long first_run[CBX_MAX_FAMILIES + 1];
+    unsigned long long* work_counter; /* [CBX_MAX_FAMILIES] */
+    int n_families;
+    int reserved;
+} cbx_hetero_args;
+
 #endif /* CBX_ARGS_H */

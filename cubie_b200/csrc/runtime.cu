@@ -24,7 +24,7 @@
 struct cbx_module {
     CUmodule module;
     CUcontext context;
-    CUfunction fn[2];
+    CUfunction fn[3];  // plain, persistent, hetero (NULL when the module has none)
     int device;
     int sm_count;
     // discrete-adjoint kernels, resolved on first use (modules generated
@@ -33,6 +33,7 @@ struct cbx_module {
     size_t lane_bytes;
     size_t record_bytes;
     bool adj_resolved;
+    int n_families;  // families of the heterogeneous kernel (0 without one)
 };
 
 namespace {
@@ -236,14 +237,22 @@ int cbx_module_load(const void* cubin, size_t cubin_size, int device, cbx_module
         delete m;
         return rc;
     }
-    const char* names[2] = {"cbx_integrate_plain", "cbx_integrate_persistent"};
-    for (int k = 0; k < 2; ++k) {
-        rc = check_cu(g_drv.cuModuleGetFunction(&m->fn[k], m->module, names[k]), names[k]);
-        if (rc) {
-            g_drv.cuModuleUnload(m->module);
-            delete m;
-            return rc;
-        }
+    const char* names[3] = {"cbx_integrate_plain", "cbx_integrate_persistent", "cbx_integrate_hetero"};
+    int found = 0;
+    for (int k = 0; k < 3; ++k) {
+        if (g_drv.cuModuleGetFunction(&m->fn[k], m->module, names[k]) != CUDA_SUCCESS) m->fn[k] = nullptr;
+        else ++found;
+    }
+    if (!found) {
+        g_drv.cuModuleUnload(m->module);
+        delete m;
+        return fail(CBX_ERR_ARGUMENT, "the cubin defines none of the integration kernels");
+    }
+    if (m->fn[CBX_KERNEL_HETERO]) {
+        CUdeviceptr probe = 0;
+        size_t fams = 0;
+        if (g_drv.cuModuleGetGlobal(&probe, &fams, m->module, "cbx_hetero_probe") == CUDA_SUCCESS)
+            m->n_families = (int)fams;
     }
     CUdevice dev;
     g_drv.cuDeviceGet(&dev, device);
@@ -275,7 +284,8 @@ int cbx_module_destroy(cbx_module* module) {
 
 int cbx_kernel_info(cbx_module* module, int kernel, int* registers, int* local_bytes, int* max_threads,
                     int* shared_bytes) {
-    if (!module || kernel < 0 || kernel > 1) return fail(CBX_ERR_ARGUMENT, "bad module or kernel index");
+    if (!module || kernel < 0 || kernel > 2 || !module->fn[kernel])
+        return fail(CBX_ERR_ARGUMENT, "bad module or kernel index (or the module has no such kernel)");
     CUfunction f = module->fn[kernel];
     int v = 0;
     if (registers && !g_drv.cuFuncGetAttribute(&v, CU_FUNC_ATTRIBUTE_NUM_REGS, f)) *registers = v;
@@ -286,7 +296,7 @@ int cbx_kernel_info(cbx_module* module, int kernel, int* registers, int* local_b
 }
 
 int cbx_occupancy(cbx_module* module, int kernel, int block, int* blocks_per_sm) {
-    if (!module || kernel < 0 || kernel > 1 || block <= 0 || !blocks_per_sm)
+    if (!module || kernel < 0 || kernel > 2 || !module->fn[kernel] || block <= 0 || !blocks_per_sm)
         return fail(CBX_ERR_ARGUMENT, "bad occupancy query");
     return check_cu(g_drv.cuOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, module->fn[kernel], block, 0),
                     "cuOccupancyMaxActiveBlocksPerMultiprocessor");
@@ -296,6 +306,7 @@ int cbx_solve(cbx_module* module, const cbx_solve_args* args, int kernel, int bl
     if (!module || !args) return fail(CBX_ERR_ARGUMENT, "null module or args");
     if (kernel != CBX_KERNEL_PLAIN && kernel != CBX_KERNEL_PERSISTENT)
         return fail(CBX_ERR_ARGUMENT, "unknown kernel kind %d", kernel);
+    if (!module->fn[kernel]) return fail(CBX_ERR_ARGUMENT, "the module has no kernel of kind %d", kernel);
     if (block <= 0 || block > 1024 || (block % 32) != 0)
         return fail(CBX_ERR_ARGUMENT, "block size %d must be a positive multiple of 32 <= 1024", block);
     if (args->n_runs < 0 || args->run_stride < args->n_runs)
@@ -348,6 +359,55 @@ int cbx_device_info(int device, int* sm_count, int* cc_major, int* cc_minor) {
 }
 
 }  // extern "C"
+
+extern "C" int cbx_solve_hetero(cbx_module* module, const cbx_hetero_args* args, int block, int grid,
+                                void* stream) {
+    if (!module || !args) return fail(CBX_ERR_ARGUMENT, "null module or args");
+    if (!module->fn[CBX_KERNEL_HETERO]) return fail(CBX_ERR_ARGUMENT, "the module has no heterogeneous kernel");
+    if (block <= 0 || block > 1024 || (block % 32) != 0)
+        return fail(CBX_ERR_ARGUMENT, "block size %d must be a positive multiple of 32 <= 1024", block);
+    if (args->n_families != module->n_families)
+        return fail(CBX_ERR_ARGUMENT, "the module was generated for %d families, args has %d", module->n_families,
+                    args->n_families);
+    if (!args->work_counter) return fail(CBX_ERR_ARGUMENT, "a zeroed work_counter is required");
+    if (args->first_run[0] != 0) return fail(CBX_ERR_ARGUMENT, "first_run[0] must be 0");
+    for (int k = 0; k < args->n_families; ++k) {
+        const cbx_solve_args& f = args->family[k];
+        const long long n = args->first_run[k + 1] - args->first_run[k];
+        if (n < 0) return fail(CBX_ERR_ARGUMENT, "first_run must be non-decreasing (family %d)", k);
+        if (f.n_runs != n || f.run_stride < n)
+            return fail(CBX_ERR_ARGUMENT, "family %d: n_runs (%lld) must equal its run range (%lld) and run_stride "
+                        "must cover it", k, f.n_runs, n);
+        if (n > 0 && (!f.inits || !f.status_out))
+            return fail(CBX_ERR_ARGUMENT, "family %d: inits and status_out are required", k);
+    }
+    const long long total = args->first_run[args->n_families];
+    if (total == 0) return CBX_OK;
+    CUcontext cur = nullptr;
+    g_drv.cuCtxGetCurrent(&cur);
+    if (cur != module->context) {
+        int rc = check_cu(g_drv.cuCtxSetCurrent(module->context), "cuCtxSetCurrent");
+        if (rc) return rc;
+    }
+    long long g = grid;
+    if (g <= 0) {
+        int per_sm = 0;
+        if (g_drv.cuOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, module->fn[CBX_KERNEL_HETERO], block, 0) !=
+                CUDA_SUCCESS || per_sm <= 0)
+            per_sm = 1;
+        g = (long long)per_sm * module->sm_count;
+        const long long needed = (total + block - 1) / block;
+        if (g > needed) g = needed;
+    }
+    if (g > 2147483647LL) return fail(CBX_ERR_ARGUMENT, "grid too large");
+    cbx_hetero_args local = *args;
+    // the kernel reads first_run[F] for its own family count F
+    for (int k = args->n_families + 1; k <= CBX_MAX_FAMILIES; ++k) local.first_run[k] = total;
+    void* params[] = {&local};
+    return check_cu(g_drv.cuLaunchKernel(module->fn[CBX_KERNEL_HETERO], (unsigned)g, 1, 1, (unsigned)block, 1, 1, 0,
+                                         static_cast<CUstream>(stream), params, nullptr),
+                    "cuLaunchKernel");
+}
 
 // ---------------------------------------------------------------------------
 // Discrete adjoint launches.

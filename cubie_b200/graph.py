@@ -57,30 +57,35 @@ class GraphSolve:
         else:
             self.grid = (self.n_runs + self.block - 1) // self.block
         # pinned host staging and device buffers
-        self.inits_h = torch.empty((n, self.n_runs), dtype=tdt).pin_memory()
+        # staging starts zeroed: horizons of 0 end every run at once
+        self.inits_h = torch.zeros((n, self.n_runs), dtype=tdt).pin_memory()
         self.params_h = torch.zeros((npar, self.n_runs), dtype=tdt).pin_memory()
-        self.inits_d = torch.empty((n, self.n_runs), dtype=tdt, device=dev)
+        self.inits_d = torch.zeros((n, self.n_runs), dtype=tdt, device=dev)
         self.params_d = torch.zeros((npar, self.n_runs), dtype=tdt, device=dev)
-        self.dur_h = torch.empty((self.n_runs,), dtype=torch.float64).pin_memory() if per_run_durations else None
-        self.dur_d = torch.empty((self.n_runs,), dtype=torch.float64, device=dev) if per_run_durations else None
+        self.dur_h = torch.zeros((self.n_runs,), dtype=torch.float64).pin_memory() if per_run_durations else None
+        self.dur_d = torch.zeros((self.n_runs,), dtype=torch.float64, device=dev) if per_run_durations else None
         self.tol_h = torch.ones((self.n_runs,), dtype=torch.float64).pin_memory() if per_run_tol_scale else None
         self.tol_d = torch.ones((self.n_runs,), dtype=torch.float64, device=dev) if per_run_tol_scale else None
         self.bufs = bufs = solver.allocate_outputs(prep, self.n_runs, dev, tdt)
-        self.out_h = {k: torch.empty(tuple(v.shape), dtype=v.dtype).pin_memory()
+        self.out_h = {k: torch.zeros(tuple(v.shape), dtype=v.dtype).pin_memory()
                       for k, v in bufs.items() if v is not None and k not in ("work",)}
         self.args = solver.make_args(prep, bufs, self.inits_d, self.params_d, None, self.n_runs, duration,
                                      settling_time, t0, self.dur_d, self.tol_d)
         self.graph = torch.cuda.CUDAGraph()
         stream = torch.cuda.Stream(device=dev)
-        # one eager run on the capture stream first (module warm, lazy state settled)
+        # One eager pass on the capture stream first, so the kernel and the
+        # copy paths are loaded before capture; it takes at most one step
+        # per run, whatever the staging buffers hold.
+        warm = _native.SolveArgs.from_buffer_copy(self.args)
+        warm.max_steps = 1
         with torch.cuda.stream(stream):
-            self._body(stream)
+            self._body(stream, warm)
         stream.synchronize()
         with torch.cuda.graph(self.graph, stream=stream):
-            self._body(stream)
+            self._body(stream, self.args)
         torch.cuda.synchronize(dev)
 
-    def _body(self, stream):
+    def _body(self, stream, args):
         self.inits_d.copy_(self.inits_h, non_blocking=True)
         self.params_d.copy_(self.params_h, non_blocking=True)
         if self.dur_d is not None:
@@ -89,7 +94,7 @@ class GraphSolve:
             self.tol_d.copy_(self.tol_h, non_blocking=True)
         self.bufs["work"].zero_()
         self.bufs["totals"].zero_()
-        self.prep["module"].launch(self.args, self.kernel, self.block, self.grid, stream.cuda_stream)
+        self.prep["module"].launch(args, self.kernel, self.block, self.grid, stream.cuda_stream)
         for k, h in self.out_h.items():
             h.copy_(self.bufs[k], non_blocking=True)
 

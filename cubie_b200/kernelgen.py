@@ -17,7 +17,7 @@ and the factories it pulls in).
 from __future__ import annotations
 
 import hashlib
-from dataclasses import dataclass, field
+from dataclasses import dataclass, field, replace
 from typing import Dict, List, Optional, Sequence, Tuple
 
 import numpy as np
@@ -347,3 +347,25 @@ def generate_kernel(system: SymbolicODE, spec: KernelSpec, gen: Optional[Generat
             raise NotImplementedError("the Rosenbrock adjoint needs an autonomous system without drivers")
         lines.append("CBX_DEFINE_ADJOINT_KERNELS(cbxsys::Cfg)")
     return GeneratedKernel(source="\n".join(lines) + "\n", system=gen, spec=spec)
+
+
+def generate_hetero_kernel(families: Sequence[Tuple[SymbolicODE, KernelSpec, GeneratedSystem]]) -> str:
+    """One translation unit holding several configurations (namespaces
+    ``cbxfam0``, ``cbxfam1``, ...) and the heterogeneous persistent kernel
+    over all of them (``csrc/device/cbx_hetero.cuh``).  All families share
+    the first family's block size."""
+    if not 1 <= len(families) <= 8:
+        raise ValueError("one to eight families per heterogeneous launch")
+    block = int(families[0][1].block_size)
+    lines = ["// generated by cubie_b200.kernelgen (heterogeneous batch); do not edit"]
+    lines += DEVICE_INCLUDES
+    lines.append('#include "cbx_hetero.cuh"')
+    names = []
+    for k, (system, spec, gen) in enumerate(families):
+        ns = f"cbxfam{k}"
+        names.append(f"{ns}::Cfg")
+        lines.append(f"namespace {ns} {{")
+        lines += family_block(system, replace(spec, block_size=block, adjoint=False), gen, ns)
+        lines.append(f"}}  // namespace {ns}")
+    lines.append(f"CBX_DEFINE_HETERO_KERNEL({block}, {', '.join(names)})")
+    return "\n".join(lines) + "\n"

@@ -26,7 +26,7 @@ extern "C" {
 
 typedef struct cbx_module cbx_module;
 
-enum cbx_kernel_kind { CBX_KERNEL_PLAIN = 0, CBX_KERNEL_PERSISTENT = 1 };
+enum cbx_kernel_kind { CBX_KERNEL_PLAIN = 0, CBX_KERNEL_PERSISTENT = 1, CBX_KERNEL_HETERO = 2 };
 
 enum cbx_error {
     CBX_OK = 0,
@@ -57,8 +57,9 @@ int cbx_compile(const char* source, const char* name, const char* const* options
                 void** cubin, size_t* cubin_size, char* log, size_t log_len);
 void cbx_free(void* p);
 
-/* Load a cubin on ``device`` (primary context) and resolve the
- * integration kernels cbx_integrate_plain and cbx_integrate_persistent. */
+/* Load a cubin on ``device`` (primary context) and resolve whichever of
+ * the integration kernels cbx_integrate_plain, cbx_integrate_persistent
+ * and cbx_integrate_hetero it defines (at least one). */
 int cbx_module_load(const void* cubin, size_t cubin_size, int device, cbx_module** module);
 
 /* cbx_compile + cbx_module_load. */
@@ -83,6 +84,13 @@ int cbx_occupancy(cbx_module* module, int kernel, int block, int* blocks_per_sm)
  * zeroed device counter).  Asynchronous on ``stream``. */
 int cbx_solve(cbx_module* module, const cbx_solve_args* args, int kernel, int block, int grid,
               void* stream);
+
+/* Several configurations in one persistent work-stealing launch (module
+ * generated for a list of families; layout in cbx_args.h).  No counterpart
+ * in the reference, which launches one kernel per system.  Requires
+ * args->work_counter to point at CBX_MAX_FAMILIES zeroed 64-bit counters;
+ * grid = 0 picks a resident grid.  Asynchronous on ``stream``. */
+int cbx_solve_hetero(cbx_module* module, const cbx_hetero_args* args, int block, int grid, void* stream);
 
 /* Device facts used for launch geometry. */
 int cbx_device_info(int device, int* sm_count, int* cc_major, int* cc_minor);

@@ -53,11 +53,27 @@ extern "C" long long emu_lane_bytes() { return (long long)sizeof(cbx_lane_probe)
 extern "C" long long emu_record_bytes() { return (long long)sizeof(cbx_seg_record_probe); }
 """
 
+HETERO_DRIVER = r"""
+cbx_dim3 threadIdx, blockIdx, blockDim, gridDim;
+extern "C" void emu_hetero(cbx_hetero_args* h, int grid, int block) {
+    blockDim = {(unsigned)block, 1, 1};
+    gridDim = {(unsigned)grid, 1, 1};
+    for (int b = 0; b < grid; ++b) {
+        for (int t = 0; t < block; ++t) {
+            blockIdx = {(unsigned)b, 0, 0};
+            threadIdx = {(unsigned)t, 0, 0};
+            cbx_integrate_hetero(*h);
+        }
+    }
+}
+"""
+
 _cache = {}
 
 
 def compile_emulated(source: str):
-    h = hashlib.sha256((source + (HERE / "cbx_host_emu.h").read_text()).encode())
+    h = hashlib.sha256((source + (HERE / "cbx_host_emu.h").read_text() + DRIVER + ADJOINT_DRIVER +
+                        HETERO_DRIVER).encode())
     for f in sorted(Path(DEVICE).glob("*")):
         h.update(f.read_bytes())
     key = h.hexdigest()[:20]
@@ -68,12 +84,17 @@ def compile_emulated(source: str):
     src = d / f"{key}.cpp"
     so = d / f"{key}.so"
     if not so.exists():
-        src.write_text(source + DRIVER + (ADJOINT_DRIVER if "CBX_DEFINE_ADJOINT_KERNELS" in source else ""))
+        hetero = "CBX_DEFINE_HETERO_KERNEL(" in source
+        src.write_text(source + ("" if hetero else DRIVER) + (HETERO_DRIVER if hetero else "") +
+                       (ADJOINT_DRIVER if "CBX_DEFINE_ADJOINT_KERNELS(" in source else ""))
         cmd = ["g++", "-O1", "-std=c++17", "-shared", "-fPIC", "-include", str(HERE / "cbx_host_emu.h"),
                f"-I{DEVICE}", "-x", "c++", str(src), "-o", str(so)]
         subprocess.run(cmd, check=True, capture_output=True, text=True)
     lib = ctypes.CDLL(str(so))
-    lib.emu_launch.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    if "CBX_DEFINE_HETERO_KERNEL(" in source:
+        lib.emu_hetero.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
+    else:
+        lib.emu_launch.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
     if "CBX_DEFINE_ADJOINT_KERNELS" in source:
         lib.emu_adjoint.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
         lib.emu_lane_bytes.restype = ctypes.c_longlong
@@ -203,3 +224,48 @@ def run_emulated_adjoint(solver, inits, params, duration, grad_state_fn, ckpt_ev
     work[:] = 0
     lib.emu_adjoint(ctypes.byref(a), ctypes.byref(g), 1, 1, 32)
     return state, status, gi, gp[:npar]
+
+
+def run_emulated_hetero(hetero, batches):
+    """The heterogeneous kernel of a HeteroSolver on the CPU; returns one
+    output dict per family (``state``, ``status``, ``totals``)."""
+    from cubie_b200 import _native
+    from cubie_b200.kernelgen import generate_hetero_kernel
+    preps, outs, keep = [], [], []
+    h = _native.HeteroArgs()
+    first = [0]
+    for k, (s, b) in enumerate(zip(hetero.solvers, batches)):
+        prep = s.prepare(float(b["duration"]), durations=b.get("durations"), load=False)
+        p = s.precision
+        inits = np.ascontiguousarray(b["initial_values"], dtype=p)
+        params = np.ascontiguousarray(b["parameters"], dtype=p)
+        n = inits.shape[1]
+        spec = prep["spec"]
+        width = (len(spec.saved_state_indices) if spec.save_state else 0) + (1 if spec.save_time else 0)
+        state = np.zeros((prep["n_save"], width, n), p)
+        status = np.zeros((n,), np.int32)
+        totals = np.zeros((4,), np.uint64)
+        durs = None if b.get("durations") is None else np.ascontiguousarray(b["durations"], np.float64)
+        a = _native.SolveArgs()
+        a.inits, a.params = inits.ctypes.data, params.ctypes.data
+        a.state_out, a.status_out, a.totals = state.ctypes.data, status.ctypes.data, totals.ctypes.data
+        a.durations = durs.ctypes.data if durs is not None else None
+        a.n_runs = a.run_stride = n
+        a.max_steps = int(s.max_steps)
+        a.duration = float(b["duration"])
+        a.save_stop, a.summary_stop = float(prep["save_stop"]), float(prep["summary_stop"])
+        a.n_save_rows, a.n_summary_rows = int(prep["n_save"]), int(prep["n_summ"])
+        h.family[k] = a
+        first.append(first[-1] + n)
+        preps.append(prep)
+        outs.append(dict(state=state, status=status, totals=totals))
+        keep += [inits, params, durs]
+    for k in range(9):
+        h.first_run[k] = first[min(k, len(first) - 1)]
+    work = np.zeros((8,), np.uint64)
+    h.work_counter = work.ctypes.data
+    h.n_families = len(hetero.solvers)
+    src = generate_hetero_kernel([(s.system, pr["spec"], pr["gen"].system) for s, pr in zip(hetero.solvers, preps)])
+    lib = compile_emulated(src)
+    lib.emu_hetero(ctypes.byref(h), 1, 32)
+    return outs

@@ -1,0 +1,61 @@
+"""Batching on the GPU: the heterogeneous launch, the CUDA-graph solve and
+the launch-shape autotuner, each against plain Solver.solve results."""
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+VDP = ["dx = y", "dy = mu * (1 - x**2) * y - x"]
+
+
+def test_hetero_launch_matches_separate_solves(cuda_device):
+    from test_hetero_emulated import families
+    from cubie_b200.hetero import HeteroSolver
+    solvers, batches = families()
+    hs = HeteroSolver(solvers)
+    results = hs.solve(batches, nan_error_trajectories=False)
+    for s, b, r in zip(solvers, batches, results):
+        ref = s.solve(b["initial_values"], b["parameters"], duration=b["duration"], durations=b["durations"],
+                      nan_error_trajectories=False)
+        assert r.status_codes.tolist() == ref.status_codes.tolist()
+        np.testing.assert_array_equal(r.state, ref.state)
+        assert r.totals == ref.totals
+
+
+def _vdp_solver(**kw):
+    from cubie_b200 import Solver, create_ODE_system
+    sysm = create_ODE_system(VDP, states={"x": 2.0, "y": 0.0}, parameters={"mu": 10.0}, precision=np.float32)
+    return Solver(sysm, algorithm="ros3p", rtol=1e-6, atol=1e-6, linear_correction_type="gmres",
+                  preconditioner_type=None, mixed_precision=True, output_types=["state"], **kw)
+
+
+def test_graph_solve_matches_solve_on_two_calls(cuda_device):
+    solver = _vdp_solver()
+    n = 3000
+    g = solver.graph(n, 200.0, per_run_durations=True)
+    for seed in (1, 2):
+        rng = np.random.default_rng(seed)
+        mu = 10.0 ** rng.uniform(0, 2, n)
+        x0 = rng.uniform(-2, 2, (2, n))
+        out = g(x0, mu[None, :], 2 * mu)
+        ref = solver.solve(x0, mu[None, :], duration=200.0, durations=2 * mu, nan_error_trajectories=False)
+        np.testing.assert_array_equal(out["status"].numpy(), ref.status_codes)
+        np.testing.assert_array_equal(out["state"].numpy(), ref.state)
+        assert int(out["totals"][0]) == ref.totals["steps"]
+
+
+def test_autotuned_solver_matches_default(cuda_device, tmp_path, monkeypatch):
+    monkeypatch.setenv("CUBIE_B200_CACHE_DIR", str(tmp_path))
+    rng = np.random.default_rng(3)
+    n = 4096
+    mu = 10.0 ** rng.uniform(0, 2, n)
+    x0 = rng.uniform(-2, 2, (2, n))
+    auto = _vdp_solver(block_size="auto")
+    r = auto.solve(x0, mu[None, :], duration=200.0, durations=2 * mu, nan_error_trajectories=False)
+    assert not auto.autotune_pending and auto.block_size in (32, 64, 128, 256)
+    assert len(auto.autotune_result["timings_ms"]) >= 4
+    ref = _vdp_solver().solve(x0, mu[None, :], duration=200.0, durations=2 * mu, nan_error_trajectories=False)
+    assert r.status_codes.tolist() == ref.status_codes.tolist()
+    err = np.abs(r.state - ref.state) / (1e-6 + 1e-6 * np.abs(ref.state))
+    assert float(np.max(err)) < 1e-3
