@@ -421,6 +421,88 @@ def hetero_arm(args, dev):
             "families": fam, "graph": True}
 
 
+def hh_cable(nc):
+    """Equations of an nc-compartment Hodgkin-Huxley cable (states V, m, h,
+    n per compartment, grouped by variable; parameters gNa, gK, gc; driver
+    I injected into compartment 0; sealed ends)."""
+    V = [f"V{j:02d}" for j in range(nc)]
+    eqs = []
+    for j in range(nc):
+        v, m, h, n = V[j], f"m{j:02d}", f"h{j:02d}", f"n{j:02d}"
+        left = V[j - 1] if j > 0 else v
+        right = V[j + 1] if j < nc - 1 else v
+        inj = "I + " if j == 0 else ""
+        eqs.append(f"d{v} = {inj}gc * ({left} - 2 * {v} + {right}) - gNa * {m}**3 * {h} * ({v} - 50.0)"
+                   f" - gK * {n}**4 * ({v} + 77.0) - 0.3 * ({v} + 54.4)")
+    for j in range(nc):
+        v, m = V[j], f"m{j:02d}"
+        eqs.append(f"d{m} = 0.1 * ({v} + 40.0) / (1 - exp(-({v} + 40.0) / 10.0)) * (1 - {m})"
+                   f" - 4.0 * exp(-({v} + 65.0) / 18.0) * {m}")
+    for j in range(nc):
+        v, h = V[j], f"h{j:02d}"
+        eqs.append(f"d{h} = 0.07 * exp(-({v} + 65.0) / 20.0) * (1 - {h}) - 1.0 / (1 + exp(-({v} + 35.0) / 10.0)) * {h}")
+    for j in range(nc):
+        v, n = V[j], f"n{j:02d}"
+        eqs.append(f"d{n} = 0.01 * ({v} + 55.0) / (1 - exp(-({v} + 55.0) / 10.0)) * (1 - {n})"
+                   f" - 0.125 * exp(-({v} + 65.0) / 80.0) * {n}")
+    states = {**{f"V{j:02d}": -65.0 for j in range(nc)}, **{f"m{j:02d}": 0.05 for j in range(nc)},
+              **{f"h{j:02d}": 0.6 for j in range(nc)}, **{f"n{j:02d}": 0.32 for j in range(nc)}}
+    return eqs, states, {"gNa": 120.0, "gK": 36.0, "gc": 0.5}, ["I"]
+
+
+def cable_arm(args, dev):
+    """Hodgkin-Huxley cable: 64 compartments x (V, m, h, n) = 256 states;
+    per run gNa~U[80,160], gK~U[20,50], coupling~U[0.1,1]; a step current
+    (10 for t < 5, then 0) from a 1000-point sample array through the array
+    interpolator (cubic, clamped); l_stable_dirk_3 (no embedded error
+    estimate, so fixed steps of 0.025) with Newton + BiCGSTAB at rtol =
+    atol = 1e-4; FP32 stepping with FP64 time and control; summaries only
+    (mean V, max V and peaks[3] of every compartment, sampled every 0.1)
+    over t in [0, 10]; one warp per run.  Accuracy: the summaries against
+    an FP64 solve with the same method, step and tolerances on 256 of the
+    runs."""
+    import torch
+    from cubie_b200 import Solver, create_ODE_system
+    nc, n, T = 64, args.c3_n, 10.0
+    eqs, states, params, drivers = hh_cable(nc)
+    rng = np.random.default_rng(3)
+    x0 = np.tile(np.array(list(states.values()))[:, None], (1, n))
+    p = np.stack([rng.uniform(80, 160, n), rng.uniform(20, 50, n), rng.uniform(0.1, 1.0, n)])
+    t_s = np.arange(1000) * 0.01
+    drv = {"driver_sample_period": 0.01, "t0": 0.0, "order": 3, "wrap": False, "I": np.where(t_s < 5.0, 10.0, 0.0)}
+    kw = dict(algorithm="l_stable_dirk_3", linear_correction_type="bicgstab", layout="warp", dt=0.025,
+              output_types=["mean", "max", "peaks[3]"], summarise_every=T, sample_summaries_every=0.1,
+              summarise_variables=[f"V{j:02d}" for j in range(nc)], device=dev.index, max_steps=100000)
+    sys32 = create_ODE_system(eqs, states=states, parameters=params, drivers=drivers, precision=np.float32)
+    # FP32 stepping needs Newton tolerances above its rounding floor (a
+    # +-65 mV state rounds at ~4e-6): rtol = atol = 1e-4 on both solves
+    kw.update(rtol=1e-4, atol=1e-4)
+    s32 = Solver(sys32, mixed_precision=True, **kw)
+    s32.solve(x0[:, :64], p[:, :64], drivers=drv, duration=T, nan_error_trajectories=False)   # compile, warm
+    times = []
+    for _ in range(args.c3_steps):
+        r = s32.solve(torch.as_tensor(x0, device=dev).float(), torch.as_tensor(p, device=dev).float(),
+                      drivers=drv, duration=T, nan_error_trajectories=False)
+        times.append(s32.last_kernel_ms)
+    K = min(256, n)
+    sys64 = create_ODE_system(eqs, states=states, parameters=params, drivers=drivers, precision=np.float64)
+    r64 = Solver(sys64, **kw).solve(x0[:, :K], p[:, :K], drivers=drv, duration=T, nan_error_trajectories=False)
+    a, b = r.state_summaries[:, :, :K].astype(np.float64), r64.state_summaries
+    mean_max = np.concatenate([a[:, 0::5], a[:, 1::5]], axis=1), np.concatenate([b[:, 0::5], b[:, 1::5]], axis=1)
+    err = np.max(np.abs(mean_max[0] - mean_max[1]) / (1e-3 + 1e-4 * np.abs(mean_max[1])), axis=(0, 1))
+    ok = (r.status_codes[:K] == 0) & (r64.status_codes == 0) & (err <= SOLVED_TOL_UNITS)
+    ms = float(np.mean(times))
+    frac = float(np.mean(ok))
+    return {"workload": "HH cable 64 x (V,m,h,n) = 256 states, 65,536 runs, l_stable_dirk_3 fixed dt 0.025 + Newton "
+                        "+ BiCGSTAB (rtol=atol=1e-4), step current from a 1000-point array, t in [0,10], summaries "
+                        "mean/max/peaks[3] of every V, FP32 + FP64 control, one warp per run",
+            "n_systems": n, "ms": ms, "value": n * float(np.mean(r.status_codes == 0)) * frac / (ms * 1e-3),
+            "unit": "systems/s", "status_ok_fraction": float(np.mean(r.status_codes == 0)),
+            "matched_fraction_vs_fp64_same_method": frac,
+            "summary_error_units_pct50_90_99": [float(np.percentile(err, q)) for q in (50, 90, 99)],
+            "totals": r.totals, "note": "error units: 1e-3 + 1e-4 |ref| on mean and max V"}
+
+
 def plain_wave(sysm, device: int) -> int:
     """Runs in one full resident wave of the plain kernel on this GPU."""
     from cubie_b200 import Solver, _native
@@ -575,6 +657,8 @@ def gpu_arm(args, rank: int, world: int, dist):
         peaks = measured_peaks()
         lor = lorenz_arm(args, dev) if args.lorenz_n > 0 else None
         log('lorenz', lor)
+        c3 = cable_arm(args, dev) if args.c3_n > 0 else None
+        log('cable', c3)
         c5 = hetero_arm(args, dev) if args.c5_n > 0 else None
         log('hetero', c5)
         adj = adjoint_arm(args, dev) if args.adj_n > 0 else None
@@ -629,6 +713,7 @@ def gpu_arm(args, rank: int, world: int, dist):
             "adjoint": adj,
             "lorenz": lor,
             "heterogeneous": c5,
+            "cable": c3,
             "cpu_baseline": cpu,
             "clocks": clocks.summary(),
         }
@@ -670,6 +755,8 @@ def main():
     ap.add_argument("--lorenz-n", type=int, default=4096, help="Lorenz saved-trajectory leg size (0: skip)")
     ap.add_argument("--c5-n", type=int, default=1 << 20, help="heterogeneous three-system leg size (0: skip)")
     ap.add_argument("--c5-steps", type=int, default=2)
+    ap.add_argument("--c3-n", type=int, default=65536, help="Hodgkin-Huxley cable leg size (0: skip)")
+    ap.add_argument("--c3-steps", type=int, default=2)
     ap.add_argument("--adj-steps", type=int, default=3)
     ap.add_argument("--adj-warmup", type=int, default=1)
     args = ap.parse_args()

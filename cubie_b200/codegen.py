@@ -360,3 +360,22 @@ def generate_system(system: SymbolicODE, struct_name: str = "System", second_ord
                            n_params=system.num_parameters, n_drivers=system.num_drivers,
                            n_observables=system.num_observables,
                            jac_pattern=jac_pattern, pjac_pattern=pjac_pattern, flops=flops)
+
+
+def system_stub(system: SymbolicODE, struct_name: str = "System") -> GeneratedSystem:
+    """The size constants of ``system`` without any functions: the
+    warp-per-system layout evaluates the system through its class-grouped
+    code (cubie_b200/warpgen.py) and needs nothing else from the
+    straight-line struct."""
+    n = system.num_states
+    src = "\n".join([f"struct {struct_name} {{",
+                     f"    static constexpr int N = {n};",
+                     f"    static constexpr int NP = {system.num_parameters};",
+                     f"    static constexpr int ND = {system.num_drivers};",
+                     f"    static constexpr int NO = {system.num_observables};",
+                     "    static constexpr int NJ = 1;",
+                     "    static constexpr int NPJ = 1;",
+                     "};"])
+    return GeneratedSystem(name=system.name, source=src, n=n, n_params=system.num_parameters,
+                           n_drivers=system.num_drivers, n_observables=system.num_observables,
+                           jac_pattern=[], pjac_pattern=[], flops={})

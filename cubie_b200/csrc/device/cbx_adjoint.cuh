@@ -244,6 +244,8 @@ struct TransposedStageOp {
     }
     __device__ __forceinline__ C tol(int i) const { return krylov_tol<Cfg>(i, ref[i], scale); }
     __device__ __forceinline__ C wnorm2(const R* v) const { return weighted_norm2<Cfg, K>(v, ref, scale); }
+    template <class T> __device__ __forceinline__ T reduce(T partial) const { return partial; }
+    static constexpr int KT = K;
 };
 
 template <class Cfg>

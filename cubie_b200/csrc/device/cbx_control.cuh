@@ -66,7 +66,18 @@ struct Controller {
             accept = true;
             return SUCCESS;
         } else {
-            const C nrm2 = error_norm2(ynew, y, err, tol_scale);
+            return update_with_norm(dt, error_norm2(ynew, y, err, tol_scale), niters, truncated, accept, st);
+        }
+    }
+    // The same decision from an error norm computed elsewhere (the
+    // warp-per-system path reduces it over the lanes).
+    static __device__ __forceinline__ int update_with_norm(C& dt, C nrm2, int niters, bool truncated, bool& accept,
+                                                           State& st) {
+        if constexpr (Cfg::CTRL == CTRL_FIXED) {
+            accept = true;
+            return SUCCESS;
+        } else {
+            if (is_nan(nrm2) || !is_finite(nrm2)) nrm2 = C(1e16);
             accept = nrm2 <= C(1);
             const C safety = C(Cfg::CTL_SAFETY);
             C gain;

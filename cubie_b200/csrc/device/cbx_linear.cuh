@@ -6,6 +6,11 @@
 //   void precond(const R* v, R* out, R* scratch) const;  // out ~= A^-1 v
 //   C    wnorm2(const R* v) const;                // weighted mean-square norm
 //   C    tol(int i) const;                        // weight denominator of wnorm2
+//   T    reduce(T partial) const;                 // sum of a per-holder partial
+//   static constexpr int KT;                      // total width (K summed over holders)
+// where an operator held by one thread has K = system width and an
+// identity ``reduce``, and an operator whose vectors are spread over a warp
+// has K = components per lane and sums the lanes' partials.
 // where wnorm2(v) = mean_i (|v_i| / tol(i))^2 is the reference's scaled
 // norm (src/cubie/integrators/norms.py:165-196) with the Krylov atol/rtol.
 //
@@ -60,6 +65,8 @@ __device__ __forceinline__ int solve_mr(const Op& op, typename Cfg::R* rhs,
                 den += C(tmp[i]) * C(tmp[i]);
             }
         }
+        num = op.reduce(num);
+        den = op.reduce(den);
         const R alpha = (den != C(0)) ? R(num / den) : R(0);
 #pragma unroll
         for (int i = 0; i < K; ++i) {
@@ -110,6 +117,7 @@ __device__ __forceinline__ int solve_bicgstab(const Op& op, typename Cfg::R* rhs
         sq = (sq > lim) ? lim : sq;
         rho_prev += sq;
     }
+    rho_prev = op.reduce(rho_prev);
     C acc = op.wnorm2(rhs);
     bool converged = acc <= tol2;
     bool broken = false;
@@ -133,6 +141,7 @@ __device__ __forceinline__ int solve_bicgstab(const Op& op, typename Cfg::R* rhs
             v[i] = clampd(v[i], lim);
             dot_r0v += clampd(r0[i] * v[i], lim);
         }
+        dot_r0v = op.reduce(dot_r0v);
         const bool alpha_overflow = absv(rho_prev) > absv(dot_r0v) * lim;
         broken = broken || alpha_overflow;
         finished = converged || broken;
@@ -163,6 +172,8 @@ __device__ __forceinline__ int solve_bicgstab(const Op& op, typename Cfg::R* rhs
             R sq = tmp[i] * tmp[i];
             dot_tt += (sq > lim) ? lim : sq;
         }
+        dot_ts = op.reduce(dot_ts);
+        dot_tt = op.reduce(dot_tt);
         const bool omega_overflow = absv(dot_ts) > dot_tt * lim;
         const R omega = (dot_tt != R(0) && !omega_overflow) ? dot_ts / dot_tt : R(0);
         const R omega_eff = finished ? R(0) : omega;
@@ -176,6 +187,7 @@ __device__ __forceinline__ int solve_bicgstab(const Op& op, typename Cfg::R* rhs
         R rho_new = R(0);
 #pragma unroll
         for (int i = 0; i < K; ++i) rho_new += clampd(r0[i] * rhs[i], lim);
+        rho_new = op.reduce(rho_new);
         const bool rho_bad = absv(rho_new) < tiny;
         const bool omega_bad = absv(omega) < tiny;
         broken = broken || (!converged && (rho_bad || omega_bad));
@@ -222,7 +234,7 @@ __device__ __forceinline__ int solve_gmres(const Op& op, typename Cfg::R* rhs,
     R b[K], w[K], z[K];
     R wt[K], iwt[K];  // W and W^-1
     {
-        const R sK = sqrt_t(R(K));
+        const R sK = sqrt_t(R(Op::KT));  // total width: the weighted norm is a mean over every component
 #pragma unroll
         for (int i = 0; i < K; ++i) {
             iwt[i] = R(op.tol(i)) * sK;
@@ -236,7 +248,7 @@ __device__ __forceinline__ int solve_gmres(const Op& op, typename Cfg::R* rhs,
             const R u = v[i] * wt[i];
             s += u * u;
         }
-        return sqrt_t(s);
+        return sqrt_t(op.reduce(s));
     };
 
     const R tol = R(Cfg::KRYLOV_FLOOR) + R(Cfg::KRYLOV_REDUCTION) * scaled_norm(rhs);
@@ -281,6 +293,7 @@ __device__ __forceinline__ int solve_gmres(const Op& op, typename Cfg::R* rhs,
                     R dot = R(0);
 #pragma unroll
                     for (int i = 0; i < K; ++i) dot += w[i] * V[l][i];
+                    dot = op.reduce(dot);
                     hcol[l] = dot;
 #pragma unroll
                     for (int i = 0; i < K; ++i) w[i] = w[i] - dot * V[l][i];
@@ -289,7 +302,7 @@ __device__ __forceinline__ int solve_gmres(const Op& op, typename Cfg::R* rhs,
             R hn = R(0);
 #pragma unroll
             for (int i = 0; i < K; ++i) hn += w[i] * w[i];
-            hn = sqrt_t(hn);
+            hn = sqrt_t(op.reduce(hn));
             {
                 const R inv = (hn > R(0)) ? R(1) / hn : R(0);
 #pragma unroll

@@ -76,6 +76,8 @@ struct SingleStageOp {
     }
     __device__ __forceinline__ C tol(int i) const { return krylov_tol<Cfg>(i, ref[i], scale); }
     __device__ __forceinline__ C wnorm2(const R* v) const { return weighted_norm2<Cfg, K>(v, ref, scale); }
+    template <class T> __device__ __forceinline__ T reduce(T partial) const { return partial; }
+    static constexpr int KT = K;
 };
 
 // Coupled S-stage operator (A v)_i = v_i - h J_i sum_j a_ij v_j with J_i the
@@ -127,6 +129,8 @@ struct CoupledOp {
     }
     __device__ __forceinline__ C tol(int i) const { return krylov_tol<Cfg>(i, ref[i % N], scale); }
     __device__ __forceinline__ C wnorm2(const R* v) const { return weighted_norm2<Cfg, K>(v, ref, scale); }
+    template <class T> __device__ __forceinline__ T reduce(T partial) const { return partial; }
+    static constexpr int KT = K;
 };
 
 // Damped Newton iteration with NLNewton-style acceptance

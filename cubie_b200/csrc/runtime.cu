@@ -24,7 +24,7 @@
 struct cbx_module {
     CUmodule module;
     CUcontext context;
-    CUfunction fn[3];  // plain, persistent, hetero (NULL when the module has none)
+    CUfunction fn[4];  // plain, persistent, hetero, warp (NULL when the module has none)
     int device;
     int sm_count;
     // discrete-adjoint kernels, resolved on first use (modules generated
@@ -237,9 +237,10 @@ int cbx_module_load(const void* cubin, size_t cubin_size, int device, cbx_module
         delete m;
         return rc;
     }
-    const char* names[3] = {"cbx_integrate_plain", "cbx_integrate_persistent", "cbx_integrate_hetero"};
+    const char* names[4] = {"cbx_integrate_plain", "cbx_integrate_persistent", "cbx_integrate_hetero",
+                            "cbx_integrate_warp"};
     int found = 0;
-    for (int k = 0; k < 3; ++k) {
+    for (int k = 0; k < 4; ++k) {
         if (g_drv.cuModuleGetFunction(&m->fn[k], m->module, names[k]) != CUDA_SUCCESS) m->fn[k] = nullptr;
         else ++found;
     }
@@ -284,7 +285,7 @@ int cbx_module_destroy(cbx_module* module) {
 
 int cbx_kernel_info(cbx_module* module, int kernel, int* registers, int* local_bytes, int* max_threads,
                     int* shared_bytes) {
-    if (!module || kernel < 0 || kernel > 2 || !module->fn[kernel])
+    if (!module || kernel < 0 || kernel > 3 || !module->fn[kernel])
         return fail(CBX_ERR_ARGUMENT, "bad module or kernel index (or the module has no such kernel)");
     CUfunction f = module->fn[kernel];
     int v = 0;
@@ -296,7 +297,7 @@ int cbx_kernel_info(cbx_module* module, int kernel, int* registers, int* local_b
 }
 
 int cbx_occupancy(cbx_module* module, int kernel, int block, int* blocks_per_sm) {
-    if (!module || kernel < 0 || kernel > 2 || !module->fn[kernel] || block <= 0 || !blocks_per_sm)
+    if (!module || kernel < 0 || kernel > 3 || !module->fn[kernel] || block <= 0 || !blocks_per_sm)
         return fail(CBX_ERR_ARGUMENT, "bad occupancy query");
     return check_cu(g_drv.cuOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, module->fn[kernel], block, 0),
                     "cuOccupancyMaxActiveBlocksPerMultiprocessor");
@@ -304,7 +305,7 @@ int cbx_occupancy(cbx_module* module, int kernel, int block, int* blocks_per_sm)
 
 int cbx_solve(cbx_module* module, const cbx_solve_args* args, int kernel, int block, int grid, void* stream) {
     if (!module || !args) return fail(CBX_ERR_ARGUMENT, "null module or args");
-    if (kernel != CBX_KERNEL_PLAIN && kernel != CBX_KERNEL_PERSISTENT)
+    if (kernel != CBX_KERNEL_PLAIN && kernel != CBX_KERNEL_PERSISTENT && kernel != CBX_KERNEL_WARP)
         return fail(CBX_ERR_ARGUMENT, "unknown kernel kind %d", kernel);
     if (!module->fn[kernel]) return fail(CBX_ERR_ARGUMENT, "the module has no kernel of kind %d", kernel);
     if (block <= 0 || block > 1024 || (block % 32) != 0)
@@ -313,8 +314,8 @@ int cbx_solve(cbx_module* module, const cbx_solve_args* args, int kernel, int bl
         return fail(CBX_ERR_ARGUMENT, "run_stride (%lld) must be >= n_runs (%lld)", args->run_stride,
                     args->n_runs);
     if (!args->inits || !args->status_out) return fail(CBX_ERR_ARGUMENT, "inits and status_out are required");
-    if (kernel == CBX_KERNEL_PERSISTENT && !args->work_counter)
-        return fail(CBX_ERR_ARGUMENT, "the persistent kernel needs a zeroed work_counter");
+    if ((kernel == CBX_KERNEL_PERSISTENT || kernel == CBX_KERNEL_WARP) && !args->work_counter)
+        return fail(CBX_ERR_ARGUMENT, "the persistent and warp kernels need a zeroed work_counter");
     if (args->n_runs == 0) return CBX_OK;
     CUcontext cur = nullptr;
     g_drv.cuCtxGetCurrent(&cur);
@@ -332,7 +333,8 @@ int cbx_solve(cbx_module* module, const cbx_solve_args* args, int kernel, int bl
                 per_sm <= 0)
                 per_sm = 1;
             g = (long long)per_sm * module->sm_count;
-            long long needed = (args->n_runs + block - 1) / block;
+            const long long runs_per_block = kernel == CBX_KERNEL_WARP ? block / 32 : block;
+            long long needed = (args->n_runs + runs_per_block - 1) / runs_per_block;
             if (g > needed) g = needed;
         }
     }

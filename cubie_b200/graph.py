@@ -47,10 +47,13 @@ class GraphSolve:
         n, npar = solver.system.num_states, max(solver.system.num_parameters, 1)
         self.prep = prep = solver.prepare(duration, settling_time, t0,
                                           durations=np.zeros(1) if per_run_durations else None)
-        kind = kernel or solver.kernel_kind
-        self.kernel = 1 if kind == "persistent" else 0
+        self.kernel = solver.launch_kind if kernel is None else (1 if kernel == "persistent" else 0)
         self.block = int(block or solver.block_size)
-        if self.kernel == 1:
+        if self.kernel == 3:
+            per_sm = prep["module"].occupancy(3, self.block)
+            sms = _native.device_info(solver.device)["sm_count"]
+            self.grid = max(1, min(max(per_sm, 1) * sms, (self.n_runs + self.block // 32 - 1) // (self.block // 32)))
+        elif self.kernel == 1:
             per_sm = prep["module"].occupancy(1, self.block)
             sms = _native.device_info(solver.device)["sm_count"]
             self.grid = max(1, min(max(per_sm, 1) * sms, (self.n_runs + self.block - 1) // self.block))

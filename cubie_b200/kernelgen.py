@@ -100,6 +100,8 @@ class KernelSpec:
     dense_prediction: Optional[bool] = None
     # discrete adjoint kernels (forward with checkpoints, reverse sweep)
     adjoint: bool = False
+    # "thread": one run per thread; "warp": one run per warp (large systems)
+    layout: str = "thread"
 
     @property
     def adaptive(self) -> bool:
@@ -204,10 +206,12 @@ DEVICE_INCLUDES = ['#include "cbx_common.cuh"', '#include "cbx_args.h"', '#inclu
                    '#include "cbx_control.cuh"', '#include "cbx_loop.cuh"']
 
 
-def family_block(system: SymbolicODE, spec: KernelSpec, gen: GeneratedSystem, ns: str) -> List[str]:
+def family_block(system: SymbolicODE, spec: KernelSpec, gen: GeneratedSystem, ns: str,
+                 warp_source: Optional[str] = None) -> List[str]:
     """The generated pieces of one configuration (system struct, tolerance
     tables, index tables, tableau, summary metrics and ``Cfg``), to be
-    placed inside namespace ``ns``."""
+    placed inside namespace ``ns``; ``warp_source`` (the class-grouped
+    system of the warp-per-system layout) adds ``Cfg::WSys``."""
     tab = spec.tableau
     n = system.num_states
     rtype = "float" if np.dtype(spec.precision) == np.float32 else "double"
@@ -243,6 +247,8 @@ def family_block(system: SymbolicODE, spec: KernelSpec, gen: GeneratedSystem, ns
         return float(v)
 
     lines: List[str] = [gen.source]
+    if warp_source is not None:
+        lines.append(warp_source)
     tol_arrays = [("atol", spec.atol), ("rtol", spec.rtol), ("katol", katol), ("krtol", krtol), ("natol", natol),
                   ("nrtol", nrtol)]
     for name, vals in tol_arrays:
@@ -315,6 +321,7 @@ def family_block(system: SymbolicODE, spec: KernelSpec, gen: GeneratedSystem, ns
         f"    static constexpr int BLOCK = {int(spec.block_size)};",
         f"    static constexpr int MIN_BLOCKS = {max(int(spec.min_blocks_per_sm), 1)};",
         f"    using Step = {STEP_TYPES[tab.kind]};",
+        *([f"    using WSys = {ns}::WarpSystem;"] if warp_source is not None else []),
         *[f"    static __device__ __forceinline__ C {name}(int i) {{ return cbx_{name}[i]; }}" for name, _ in tol_arrays],
         "};",
     ]
@@ -322,12 +329,15 @@ def family_block(system: SymbolicODE, spec: KernelSpec, gen: GeneratedSystem, ns
     return lines
 
 
-def generate_kernel(system: SymbolicODE, spec: KernelSpec, gen: Optional[GeneratedSystem] = None) -> GeneratedKernel:
+def generate_kernel(system: SymbolicODE, spec: KernelSpec, gen: Optional[GeneratedSystem] = None,
+                    warp_code=None) -> GeneratedKernel:
     """Return the complete CUDA translation unit for ``spec``: the device
     headers, then the configuration's generated pieces in namespace
     ``cbxsys``, then the kernels instantiated for ``cbxsys::Cfg``."""
     gen = gen or generate_system(system, second_order=spec.adjoint and spec.tableau.kind == ROSENBROCK)
     tab = spec.tableau
+    if spec.layout == "warp":
+        return _generate_warp_kernel(system, spec, gen, warp_code)
     lines = ["// generated by cubie_b200.kernelgen; do not edit"]
     if int(spec.min_blocks_per_sm) > 1:
         lines.append("#define CBX_LAUNCH_BOUNDS(CFG) __launch_bounds__(CFG::BLOCK, CFG::MIN_BLOCKS)")
@@ -369,3 +379,27 @@ def generate_hetero_kernel(families: Sequence[Tuple[SymbolicODE, KernelSpec, Gen
         lines.append(f"}}  // namespace {ns}")
     lines.append(f"CBX_DEFINE_HETERO_KERNEL({block}, {', '.join(names)})")
     return "\n".join(lines) + "\n"
+
+
+def _generate_warp_kernel(system: SymbolicODE, spec: KernelSpec, gen: GeneratedSystem, warp_code=None):
+    """Translation unit of the warp-per-system layout (``cbx_integrate_warp``)."""
+    from .warpgen import generate_warp_system
+    tab = spec.tableau
+    if tab.kind != DIRK:
+        raise NotImplementedError("the warp-per-system layout runs diagonally implicit RK tableaus")
+    if spec.save_observables or spec.summarised_observable_indices:
+        raise NotImplementedError("the warp-per-system layout saves and summarises states only")
+    if spec.adjoint:
+        raise NotImplementedError("no adjoint on the warp-per-system layout")
+    if spec.block_size % 32:
+        raise ValueError("block size must be a multiple of 32")
+    warp_code = warp_code or generate_warp_system(system)
+    spec = replace(spec, dense_prediction=False)
+    lines = ["// generated by cubie_b200.kernelgen (warp-per-system layout); do not edit"]
+    lines += DEVICE_INCLUDES
+    lines.append('#include "cbx_warp.cuh"')
+    lines.append("namespace cbxsys {")
+    lines += family_block(system, spec, gen, "cbxsys", warp_source=warp_code.source)
+    lines.append("}  // namespace cbxsys")
+    lines.append("CBX_DEFINE_WARP_KERNEL(cbxsys::Cfg)")
+    return GeneratedKernel(source="\n".join(lines) + "\n", system=gen, spec=spec)

@@ -53,7 +53,7 @@ OUTPUT_KEYS = {"output_types", "saved_state_indices", "saved_observable_indices"
                "save_variables", "summarise_variables"}
 LOOP_KEYS = {"save_every", "summarise_every", "sample_summaries_every"}
 EXECUTION_KEYS = {"mixed_precision", "kernel", "block_size", "min_blocks_per_sm", "max_steps", "device", "fast_math",
-                  "precision", "adjoint"}
+                  "precision", "adjoint", "layout"}
 IGNORED_KEYS = {"memory_settings", "cache", "auto_memory", "lineinfo", "time_logging_level",
                 "profileCUDA", "cache_settings"}
 RENAMED = {"dt_save": "save_every", "dt_summarise": "summarise_every",
@@ -137,6 +137,14 @@ class Solver:
         self.block_size = 128 if self.autotune_pending else int(bs)
         self.min_blocks_per_sm = int(execution.get("min_blocks_per_sm", 1))
         self.adjoint = bool(execution.get("adjoint", False))
+        # "thread": one run per thread; "warp": one run per warp, for large
+        # systems (diagonally implicit tableaus); "auto": warp from 64 states
+        layout = execution.get("layout", "thread")
+        if layout == "auto":
+            layout = "warp" if (system.num_states >= 64 and self.tableau.kind == "dirk") else "thread"
+        if layout not in ("thread", "warp"):
+            raise ValueError("layout must be 'thread', 'warp' or 'auto'")
+        self.layout = layout
         self.max_steps = int(execution.get("max_steps", 0))
         self.device = int(execution.get("device", 0))
         self.fast_math = bool(execution.get("fast_math", True))
@@ -365,7 +373,7 @@ class Solver:
             driver_eval_start=dm.get("eval_start", 0.0), driver_inv_resolution=dm.get("inv_resolution", 1.0),
             driver_wrap=dm.get("wrap", False),
             mixed_precision=self.mixed_precision, block_size=self.block_size,
-            min_blocks_per_sm=self.min_blocks_per_sm, adjoint=self.adjoint,
+            min_blocks_per_sm=self.min_blocks_per_sm, adjoint=self.adjoint, layout=self.layout,
             dense_prediction=None if self.attempt_dense_prediction else False,
         )
 
@@ -374,10 +382,21 @@ class Solver:
         the costly step) is generated once per solver."""
         second = bool(spec.adjoint and spec.tableau.kind == "rosenbrock")
         cache = self.__dict__.setdefault("_system_code", {})
-        gen = cache.get(second)
+        key = "stub" if spec.layout == "warp" else second
+        gen = cache.get(key)
         if gen is None:
-            gen = cache[second] = generate_system(self.system, second_order=second)
-        return generate_kernel(self.system, spec, gen=gen)
+            if spec.layout == "warp":
+                from .codegen import system_stub
+                gen = cache[key] = system_stub(self.system)
+            else:
+                gen = cache[key] = generate_system(self.system, second_order=second)
+        warp = None
+        if spec.layout == "warp":
+            warp = cache.get("warp")
+            if warp is None:
+                from .warpgen import generate_warp_system
+                warp = cache["warp"] = generate_warp_system(self.system)
+        return generate_kernel(self.system, spec, gen=gen, warp_code=warp)
 
     def module_for(self, spec: KernelSpec):
         """Compile (or fetch) the NVRTC module for ``spec`` on this device."""
@@ -548,7 +567,7 @@ class Solver:
             coeff_t = torch.as_tensor(interp.coefficients.astype(self.precision), device=dev).contiguous()
         args = self.make_args(prep, bufs, inits_t, params_t, coeff_t, n_runs, duration, settling_time, t0,
                               dur_t, tol_t)
-        kernel = 1 if self.kernel_kind == "persistent" else 0
+        kernel = self.launch_kind
         s = stream if stream is not None else torch.cuda.current_stream(dev)
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
@@ -558,6 +577,13 @@ class Solver:
         e1.synchronize()
         self.last_kernel_ms = e0.elapsed_time(e1)
         return self.collect(prep, bufs, n_runs, duration, settling_time, t0, nan_error_trajectories, on_device)
+
+    @property
+    def launch_kind(self) -> int:
+        """C-ABI kernel kind of this solver's launch (CBX_KERNEL_*)."""
+        if self.layout == "warp":
+            return 3
+        return 1 if self.kernel_kind == "persistent" else 0
 
     def graph(self, n_runs: int, duration: float, **kwargs):
         """A :class:`~cubie_b200.graph.GraphSolve`: this solve captured as

@@ -26,7 +26,7 @@ extern "C" {
 
 typedef struct cbx_module cbx_module;
 
-enum cbx_kernel_kind { CBX_KERNEL_PLAIN = 0, CBX_KERNEL_PERSISTENT = 1, CBX_KERNEL_HETERO = 2 };
+enum cbx_kernel_kind { CBX_KERNEL_PLAIN = 0, CBX_KERNEL_PERSISTENT = 1, CBX_KERNEL_HETERO = 2, CBX_KERNEL_WARP = 3 };
 
 enum cbx_error {
     CBX_OK = 0,
@@ -58,8 +58,8 @@ int cbx_compile(const char* source, const char* name, const char* const* options
 void cbx_free(void* p);
 
 /* Load a cubin on ``device`` (primary context) and resolve whichever of
- * the integration kernels cbx_integrate_plain, cbx_integrate_persistent
- * and cbx_integrate_hetero it defines (at least one). */
+ * the integration kernels cbx_integrate_plain, cbx_integrate_persistent,
+ * cbx_integrate_hetero and cbx_integrate_warp it defines (at least one). */
 int cbx_module_load(const void* cubin, size_t cubin_size, int device, cbx_module** module);
 
 /* cbx_compile + cbx_module_load. */
@@ -80,7 +80,8 @@ int cbx_occupancy(cbx_module* module, int kernel, int block, int* blocks_per_sm)
  * kernel launch (BatchSolverKernel.py:741-762).  ``args`` holds caller
  * device pointers (layouts in cbx_args.h).  grid = 0 picks
  * ceil(n_runs / block) for the plain kernel and a resident grid for the
- * persistent kernel (which also requires args->work_counter to point at a
+ * persistent kernel and for the warp-per-run kernel of large systems
+ * (CBX_KERNEL_WARP; both also require args->work_counter to point at a
  * zeroed device counter).  Asynchronous on ``stream``. */
 int cbx_solve(cbx_module* module, const cbx_solve_args* args, int kernel, int block, int grid,
               void* stream);
