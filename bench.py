@@ -591,14 +591,8 @@ def gpu_arm(args, rank: int, world: int, dist):
     ms = float(np.mean(new["times"]))
     frac, err = solved_fraction(new["y"][:, :T], new["status"][:T])
     solved_est = n * frac
-    ms_max = ms
-    total_solved = solved_est
-    if dist is not None:
-        t = torch.tensor([ms, solved_est], device=dev, dtype=torch.float64)
-        tm = t.clone()
-        dist.all_reduce(tm[:1], op=dist.ReduceOp.MAX)
-        dist.all_reduce(t[1:], op=dist.ReduceOp.SUM)
-        ms_max, total_solved = float(tm[0]), float(t[1])
+    from cubie_b200.shard import aggregate
+    ms_max, total_solved = aggregate(ms, solved_est, device=dev)
     value = total_solved / (ms_max * 1e-3)
 
     # ---- end to end through the public API with pinned host buffers
@@ -616,7 +610,8 @@ def gpu_arm(args, rank: int, world: int, dist):
         e2e_times.append(time.perf_counter() - t0)
     log('e2e', e2e_times)
     e2e_frac, _ = solved_fraction(res.state[-1][:, :T], res.status_codes[:T])
-    e2e_value = n * e2e_frac / float(np.mean(e2e_times))
+    e2e_s, e2e_solved = aggregate(float(np.mean(e2e_times)), n * e2e_frac, device=dev)
+    e2e_value = e2e_solved / e2e_s
     h2d = x0_h.numel() * 4 + mu_h.numel() * 4 + du_h.numel() * 8
     d2h = res.state.size * 4 + res.status_codes.size * 4 + 4 * 8
 
