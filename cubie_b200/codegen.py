@@ -263,11 +263,18 @@ def generate_system(system: SymbolicODE, struct_name: str = "System", second_ord
     y_map = {s: f"y[{i}]" for i, s in enumerate(system.state_symbols)}
     p_map = {s: f"p[{i}]" for i, s in enumerate(system.parameter_symbols)}
     d_map = {s: f"d[{i}]" for i, s in enumerate(system.driver_symbols)}
-    base_map = {TIME: "t", **y_map, **p_map, **d_map}
+    # Constants stay symbols through CSE and differentiation and print as
+    # literals, so ``sigma*(y - x)`` keeps its factored form (substituting
+    # the number first would let SymPy distribute it) and rounds exactly as
+    # the reference's closure-bound constants do (symbolicODE.py constants,
+    # codegen/dxdt.py constant assignments).
+    c_map = {s: f"R({float(system.constants[nm])!r})"
+             for s, nm in zip(system.constant_symbols, system.constant_names)}
+    base_map = {TIME: "t", **y_map, **p_map, **d_map, **c_map}
 
-    f = system.rhs_expressions()
-    obs = system.observable_expressions()
-    J = system.jacobian()
+    f = system.rhs_expressions(substitute_constants=False)
+    obs = system.observable_expressions(substitute_constants=False)
+    J = sp.Matrix(f).jacobian(sp.Matrix(system.state_symbols)) if n else sp.zeros(0, 0)
     jac_pattern = [(i, j) for i in range(n) for j in range(n) if J[i, j] != 0]
     # parameter Jacobian
     P = sp.Matrix(f).jacobian(sp.Matrix(system.parameter_symbols)) if system.parameter_symbols else sp.zeros(n, 0)

@@ -212,10 +212,16 @@ struct RosenbrockStep {
         else dd[0] = R(0);
         R tdv[N];
         Sys::template dfdt<R>(y, ctx.p, drv, dd, t, tdv);
+        // The proposed state starts from y and takes each stage's weighted
+        // increment in turn (or is the stage state whose row of a equals b);
+        // the error likewise, in the reference's order of operations.
+        // ``delta`` (sum of the weighted increments) feeds the compensated
+        // update of the mixed-precision mode.
 #pragma unroll
         for (int i = 0; i < N; ++i) {
             tdv[i] *= dt;
             delta[i] = R(0);
+            ynew[i] = y[i];
             if (Tab::HAS_ERR) err[i] = R(0);
         }
         R K[S][N];
@@ -265,6 +271,8 @@ struct RosenbrockStep {
                 }
                 Y[i] = v;
                 rhs[i] = corr;
+                if (!Tab::ACC_OUT && stage == Tab::B_ROW) ynew[i] = v;
+                if (Tab::HAS_ERR && !Tab::ACC_ERR && stage == Tab::BHAT_ROW) err[i] = v;
             }
             if constexpr (ND > 0) {
                 if (stage == 0) {
@@ -290,11 +298,14 @@ struct RosenbrockStep {
                 for (int j = 0; j < S; ++j)
                     if (j == stage) K[j][i] = k;
                 delta[i] += b_s * k;
-                if (Tab::HAS_ERR) err[i] += d_s * k;
+                if (Tab::ACC_OUT) ynew[i] += b_s * k;
+                if (Tab::HAS_ERR && Tab::ACC_ERR) err[i] += d_s * k;
             }
         }
+        if (Tab::HAS_ERR && !Tab::ACC_ERR) {
 #pragma unroll
-        for (int i = 0; i < N; ++i) ynew[i] = y[i] + delta[i];
+            for (int i = 0; i < N; ++i) err[i] = ynew[i] - err[i];
+        }
         if constexpr (ND > 0) Drivers<Cfg>::eval(t + dt, ctx.coeffs, drv_new);
         return status;
     }
@@ -632,7 +643,7 @@ struct DirkStep {
 #pragma unroll
                 for (int i = 0; i < N; ++i) base[i] += R(Tab::a(0, 0)) * ps.z[i];
             }
-            Sys::template dxdt<R>(base, ctx.p, drv_stage, stage_time, ps.rhs);
+            if (Tab::need_f(0)) Sys::template dxdt<R>(base, ctx.p, drv_stage, stage_time, ps.rhs);
         }
         if (Tab::DENSE_PRED && Tab::a(0, 0) == 0.0) {
 #pragma unroll
@@ -640,10 +651,13 @@ struct DirkStep {
         }
 #pragma unroll
         for (int i = 0; i < N; ++i) {
-            if (Tab::ACC_OUT) outacc[i] += R(Tab::b(0)) * ps.rhs[i];
-            else if (Tab::B_ROW == 0) ynew[i] = base[i];
+            if (Tab::ACC_OUT) {
+                if (Tab::b(0) != 0.0) outacc[i] += R(Tab::b(0)) * ps.rhs[i];
+            } else if (Tab::B_ROW == 0) ynew[i] = base[i];
             if (Tab::HAS_ERR) {
-                if (Tab::ACC_ERR) erracc[i] += R(Tab::d(0)) * ps.rhs[i];
+                if (Tab::ACC_ERR) {
+                    if (Tab::d(0) != 0.0) erracc[i] += R(Tab::d(0)) * ps.rhs[i];
+                }
                 else if (Tab::BHAT_ROW == 0) err[i] = base[i];
             }
         }
@@ -670,6 +684,9 @@ struct DirkStep {
                 if (Tab::DENSE_PRED) {
 #pragma unroll
                     for (int i = 0; i < N; ++i) ps.z[i] = ps.hist[Tab::pred_source(stage) * N + i];
+                } else if (Tab::EULER_GUESS && Tab::a(prev, prev) == 0.0) {
+#pragma unroll
+                    for (int i = 0; i < N; ++i) ps.z[i] = dt * ps.rhs[i];
                 }
                 DirkProblem<Cfg> prob;
                 prob.ctx = &ctx; prob.base = base; prob.step_start = y; prob.drv = drv_stage;
@@ -690,20 +707,23 @@ struct DirkStep {
                     stage_delta[i] += R(Tab::a(stage, stage)) * ps.z[i];
                 }
             }
-            Sys::template dxdt<R>(base, ctx.p, drv_stage, stage_time, ps.rhs);
+            if (Tab::need_f(stage)) Sys::template dxdt<R>(base, ctx.p, drv_stage, stage_time, ps.rhs);
             if (Tab::DENSE_PRED && Tab::HAS_LATER_EXPLICIT && Tab::a(stage, stage) == 0.0) {
 #pragma unroll
                 for (int i = 0; i < N; ++i) ps.hist[stage * N + i] = dt * ps.rhs[i];
             }
 #pragma unroll
             for (int i = 0; i < N; ++i) {
-                if (Tab::ACC_OUT) outacc[i] += R(Tab::b(stage)) * ps.rhs[i];
-                else if (Tab::B_ROW == stage) {
+                if (Tab::ACC_OUT) {
+                    if (Tab::b(stage) != 0.0) outacc[i] += R(Tab::b(stage)) * ps.rhs[i];
+                } else if (Tab::B_ROW == stage) {
                     ynew[i] = base[i];
                     delta[i] = stage_delta[i];
                 }
                 if (Tab::HAS_ERR) {
-                    if (Tab::ACC_ERR) erracc[i] += R(Tab::d(stage)) * ps.rhs[i];
+                    if (Tab::ACC_ERR) {
+                        if (Tab::d(stage) != 0.0) erracc[i] += R(Tab::d(stage)) * ps.rhs[i];
+                    }
                     else if (Tab::BHAT_ROW == stage) err[i] = base[i];
                 }
             }

@@ -253,14 +253,17 @@ struct WarpDirkStep {
 #pragma unroll
                 for (int i = 0; i < L; ++i) base[i] += R(Tab::a(0, 0)) * ps.z[i];
             }
-            w.rhs(base, stage_time, drv_stage, ps.rhs);
+            if (Tab::need_f(0)) w.rhs(base, stage_time, drv_stage, ps.rhs);
         }
 #pragma unroll
         for (int i = 0; i < L; ++i) {
-            if (Tab::ACC_OUT) outacc[i] += R(Tab::b(0)) * ps.rhs[i];
-            else if (Tab::B_ROW == 0) ynew[i] = base[i];
+            if (Tab::ACC_OUT) {
+                if (Tab::b(0) != 0.0) outacc[i] += R(Tab::b(0)) * ps.rhs[i];
+            } else if (Tab::B_ROW == 0) ynew[i] = base[i];
             if (Tab::HAS_ERR) {
-                if (Tab::ACC_ERR) erracc[i] += R(Tab::d(0)) * ps.rhs[i];
+                if (Tab::ACC_ERR) {
+                    if (Tab::d(0) != 0.0) erracc[i] += R(Tab::d(0)) * ps.rhs[i];
+                }
                 else if (Tab::BHAT_ROW == 0) err[i] = base[i];
             }
         }
@@ -284,6 +287,10 @@ struct WarpDirkStep {
                 base[i] = stage_delta[i] + y[i];
             }
             if (Tab::a(stage, stage) != 0.0) {
+                if (Tab::EULER_GUESS && Tab::a(prev, prev) == 0.0) {
+#pragma unroll
+                    for (int i = 0; i < L; ++i) ps.z[i] = dt * ps.rhs[i];
+                }
                 status |= stage_solve(w, base, y, drv_stage, stage_time, dt, R(Tab::a(stage, stage)), ps, its);
 #pragma unroll
                 for (int i = 0; i < L; ++i) {
@@ -291,16 +298,19 @@ struct WarpDirkStep {
                     stage_delta[i] += R(Tab::a(stage, stage)) * ps.z[i];
                 }
             }
-            w.rhs(base, stage_time, drv_stage, ps.rhs);
+            if (Tab::need_f(stage)) w.rhs(base, stage_time, drv_stage, ps.rhs);
 #pragma unroll
             for (int i = 0; i < L; ++i) {
-                if (Tab::ACC_OUT) outacc[i] += R(Tab::b(stage)) * ps.rhs[i];
-                else if (Tab::B_ROW == stage) {
+                if (Tab::ACC_OUT) {
+                    if (Tab::b(stage) != 0.0) outacc[i] += R(Tab::b(stage)) * ps.rhs[i];
+                } else if (Tab::B_ROW == stage) {
                     ynew[i] = base[i];
                     delta[i] = stage_delta[i];
                 }
                 if (Tab::HAS_ERR) {
-                    if (Tab::ACC_ERR) erracc[i] += R(Tab::d(stage)) * ps.rhs[i];
+                    if (Tab::ACC_ERR) {
+                        if (Tab::d(stage) != 0.0) erracc[i] += R(Tab::d(stage)) * ps.rhs[i];
+                    }
                     else if (Tab::BHAT_ROW == stage) err[i] = base[i];
                 }
             }

@@ -157,6 +157,9 @@ def tableau_struct(tab: Tableau, precision, dense: bool) -> str:
     diag = np.diag(a)
     later_explicit = bool(np.any(diag[1:] == 0.0)) if s > 1 else False
     out.append(f"    static constexpr bool HAS_LATER_EXPLICIT = {str(later_explicit).lower()};")
+    out.append(f"    static constexpr bool EULER_GUESS = {str(bool(tab.euler_guess)).lower()};")
+    out.append(f"    static __host__ __device__ constexpr bool need_f(int i) {{ constexpr bool v[{s}] = {{"
+               + ", ".join(str(tab.stage_derivative_needed(i)).lower() for i in range(s)) + "}; return v[i]; }")
     out.append(f"    static constexpr int PRED_FIRST = {1 if first_explicit else 0};")
     if dense:
         coeffs = tab.prediction_coefficients()

@@ -124,9 +124,6 @@ class Solver:
                 unknown.append(k)
         if unknown:
             raise KeyError(f"Unrecognized keyword arguments: {set(unknown)}")
-        if algorithm == "euler":
-            raise NotImplementedError("the explicit Euler step is not part of this engine; "
-                                      "use an explicit RK tableau such as 'heun-21' or 'dormand-prince-54'")
         self.tableau = resolve_algorithm(algorithm)
         self.mixed_precision = bool(execution.get("mixed_precision", False))
         self.kernel_kind = execution.get("kernel", "persistent")

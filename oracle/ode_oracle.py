@@ -30,6 +30,7 @@ from __future__ import annotations
 
 import math
 from dataclasses import dataclass
+from pathlib import Path
 from typing import Dict, List, Optional, Sequence
 
 import numpy as np
@@ -53,6 +54,9 @@ class OTab:
     gamma_stages: Optional[np.ndarray] = None
     dense32: float = 0.0
     dense64: float = 0.0
+    # DIRK: an implicit stage after an explicit one starts Newton from h
+    # times that stage's derivative (explicit Euler predictor)
+    euler_guess: bool = False
 
     @property
     def s(self):
@@ -143,6 +147,49 @@ TABLEAUS: Dict[str, OTab] = {
 }
 TABLEAUS["radau"] = TABLEAUS["radau_iia_5"]
 TABLEAUS["rk45"] = TABLEAUS["dormand-prince-54"]
+
+# The reference's single-purpose steps, restated as tableaus:
+#   explicit Euler (explicit_euler.py: y + h f(t, y));
+#   backward Euler (backwards_euler.py: z = h f(t + h, y + z), Newton seeded
+#   with the previous step's increment);
+#   backward Euler with an explicit Euler predictor
+#   (backwards_euler_predict_correct.py: Newton seeded with h f(t, y));
+#   Crank-Nicolson (crank_nicolson.py: trapezoidal solve seeded with h f(t, y),
+#   then a backward Euler solve seeded with the trapezoidal increment; the
+#   error is their difference).
+TABLEAUS["euler"] = _tab("erk", [[0]], [1.0], [0.0], 1)
+TABLEAUS["backwards_euler"] = _tab("dirk", [[1.0]], [1.0], [1.0], 1)
+TABLEAUS["backwards_euler_pc"] = _tab("dirk", [[0, 0], [0, 1.0]], [0.0, 1.0], [0.0, 1.0], 1, euler_guess=True)
+TABLEAUS["crank_nicolson"] = _tab("dirk", [[0, 0, 0], [0.5, 0.5, 0], [0, 0, 1.0]], [0.5, 0.5, 0.0],
+                                  [0.0, 1.0, 1.0], 2, b_hat=[0.0, 0.0, 1.0], euler_guess=True)
+
+
+def load_reference_tableaus(path) -> int:
+    """Add every tableau of a coefficient file written from the reference's
+    registries (``tests/golden/make_tableau_fixture.py``: ``<alias>/a``,
+    ``/b``, ``/c``, ``/b_hat``, ``/C``, ...) whose alias is not restated
+    above; returns the number added."""
+    data = np.load(path)
+    aliases = sorted({k.split("/")[0] for k in data.files})
+    added = 0
+    for al in aliases:
+        if al in TABLEAUS:
+            continue
+        g = lambda f: data[f"{al}/{f}"] if f"{al}/{f}" in data.files else None
+        kind = str(g("kind"))
+        kw = dict(dense32=float(g("dense32")), dense64=float(g("dense64")))
+        if g("b_hat") is not None:
+            kw["b_hat"] = g("b_hat")
+        if kind == "rosenbrock":
+            kw.update(C=g("C"), gamma=float(g("gamma")), gamma_stages=g("gamma_stages"))
+        TABLEAUS[al] = _tab(kind, g("a"), g("b"), g("c"), int(g("order")), **kw)
+        added += 1
+    return added
+
+
+_REFERENCE_TABLEAUS = Path(__file__).resolve().parent.parent / "tests" / "golden" / "ref_tableaus.npz"
+if _REFERENCE_TABLEAUS.exists():
+    load_reference_tableaus(_REFERENCE_TABLEAUS)
 
 FAMILY_CONTROLLER = {
     "erk": dict(step_controller="pi", kp=0.7, ki=-0.4, deadband_min=1.0, deadband_max=1.0,
@@ -950,14 +997,24 @@ def integrate(system: OracleSystem, algorithm: str, inits: np.ndarray, params: n
             x, st, li = lin_solve(A, Pc, nrm, rhs, ros_guess.copy())
             step_status |= st
             Ks.append(x)
+            # generic_rosenbrock_w.py:526-745: the proposed state starts at y
+            # and takes each weighted increment in turn, or is the stage state
+            # whose row of a equals b; the error likewise
+            brow = tab.row_match(tab.b)
+            bhrow = tab.row_match(tab.b_hat)
             delta = x * rt(tab.b[0])
-            err = x * rt(tab.d[0])
+            ynew = Y + rt(tab.b[0]) * x if brow is None else Y.copy()
+            err = x * rt(tab.d[0]) if bhrow is None else np.zeros_like(Y)
             for stage in range(1, s):
                 st_time = tt + h * rt(tab.c[stage])
                 Ys = Y.copy()
                 for j in range(stage):
                     if tab.a[stage, j] != 0.0:
                         Ys = Ys + rt(tab.a[stage, j]) * Ks[j]
+                if stage == brow:
+                    ynew = Ys.copy()
+                if stage == bhrow:
+                    err = Ys.copy()
                 fs = system.f(st_time, Ys, P)
                 corr = np.zeros((B, n), rt)
                 for j in range(stage):
@@ -969,9 +1026,13 @@ def integrate(system: OracleSystem, algorithm: str, inits: np.ndarray, params: n
                 step_status |= st
                 Ks.append(x)
                 delta = delta + rt(tab.b[stage]) * x
-                err = err + rt(tab.d[stage]) * x
+                if brow is None:
+                    ynew = ynew + rt(tab.b[stage]) * x
+                if bhrow is None:
+                    err = err + rt(tab.d[stage]) * x
             ros_guess = np.where(act[:, None], Ks[-1], ros_guess)
-            ynew = Y + delta
+            if tab.has_err and bhrow is not None:
+                err = ynew - err
         elif tab.kind == "firk":
             U = firk_u.copy()
             if dense:
@@ -1099,6 +1160,8 @@ def integrate(system: OracleSystem, algorithm: str, inits: np.ndarray, params: n
                             src[st_i] = latest.get(nd, st_i)
                             latest[nd] = st_i
                         z = dirk_hist[:, src[stage] * n:(src[stage] + 1) * n].copy()
+                    elif tab.euler_guess and stage > 0 and tab.a[stage - 1, stage - 1] == 0.0:
+                        z = rhs_k * h[:, None]
                     a_c = rt(aii)
                     bb = base.copy()
 
@@ -1128,6 +1191,11 @@ def integrate(system: OracleSystem, algorithm: str, inits: np.ndarray, params: n
                     base = base + a_c * z
                     sdelta = sdelta + a_c * z
                 rhs_k = system.f(st_time, base, P)
+                if dense and aii == 0.0:
+                    # an explicit stage's increment h f joins the read-ahead
+                    # history like a solved one (stage_predictors.py)
+                    dirk_hist[:, stage * n:(stage + 1) * n] = np.where(
+                        act[:, None], rhs_k * h[:, None], dirk_hist[:, stage * n:(stage + 1) * n])
                 if brow is None:
                     outacc = outacc + rt(tab.b[stage]) * rhs_k
                 elif brow == stage:

@@ -134,6 +134,73 @@ CASES = {
                                                   output_types=["state", "time"])),
 }
 
+# One case per further algorithm of the reference's registries and its
+# single-purpose steps (explicit/backward Euler, predictor-corrector,
+# Crank-Nicolson): short windows so the simulator finishes in seconds.
+_FIX = ["state", "time"]
+_ITS = ["state", "time", "iteration_counters"]
+_VDP2 = ("vdp", 2, 40, [2.0, 10.0])
+CASES.update({
+    "lorenz_euler_f64": dict(system=LORENZ, algorithm="euler", precision="float64", inputs=("lorenz", 4, 31),
+                             duration=0.2, kwargs=dict(dt=1e-3, rtol=1e-6, atol=1e-6, save_every=0.05,
+                                                       output_types=_FIX)),
+    "lorenz_ralston_f32": dict(system=LORENZ, algorithm="ralston-33", precision="float32", inputs=("lorenz", 4, 32),
+                               duration=0.2, kwargs=dict(dt=2e-3, rtol=1e-5, atol=1e-5, save_every=0.05,
+                                                         output_types=_FIX)),
+    "lorenz_rk4_f64": dict(system=LORENZ, algorithm="classical-rk4", precision="float64", inputs=("lorenz", 4, 33),
+                           duration=0.2, kwargs=dict(dt=2e-3, rtol=1e-6, atol=1e-6, save_every=0.05,
+                                                     output_types=_FIX)),
+    "lorenz_bs32_f64": dict(system=LORENZ, algorithm="bogacki-shampine-32", precision="float64",
+                            inputs=("lorenz", 4, 34), duration=0.5,
+                            kwargs=dict(rtol=1e-7, atol=1e-9, save_every=0.1, output_types=_ITS)),
+    "lorenz_cashkarp_f64": dict(system=LORENZ, algorithm="cash-karp-54", precision="float64",
+                                inputs=("lorenz", 4, 35), duration=0.5,
+                                kwargs=dict(rtol=1e-8, atol=1e-10, save_every=0.1, output_types=_ITS)),
+    "lorenz_fehlberg_f64": dict(system=LORENZ, algorithm="fehlberg-45", precision="float64",
+                                inputs=("lorenz", 4, 36), duration=0.5,
+                                kwargs=dict(rtol=1e-8, atol=1e-10, save_every=0.1, output_types=_ITS)),
+    "lorenz_tsit5_f64": dict(system=LORENZ, algorithm="tsit5", precision="float64", inputs=("lorenz", 4, 37),
+                             duration=0.5, kwargs=dict(rtol=1e-8, atol=1e-10, save_every=0.1, output_types=_ITS)),
+    "lorenz_vern7_f64": dict(system=LORENZ, algorithm="vern7", precision="float64", inputs=("lorenz", 4, 38),
+                             duration=0.5, kwargs=dict(rtol=1e-9, atol=1e-11, save_every=0.1, output_types=_ITS)),
+    "lorenz_dop853_f64": dict(system=LORENZ, algorithm="dop853", precision="float64", inputs=("lorenz", 4, 39),
+                              duration=0.5, kwargs=dict(rtol=1e-9, atol=1e-11, save_every=0.1, output_types=_ITS)),
+    "vdp_be_f64": dict(system=VDP, algorithm="backwards_euler", precision="float64", inputs=_VDP2, duration=0.5,
+                       kwargs=dict(dt=0.01, rtol=1e-6, atol=1e-6, save_every=0.125, output_types=_ITS)),
+    "vdp_bepc_f32": dict(system=VDP, algorithm="backwards_euler_pc", precision="float32",
+                         inputs=("vdp", 2, 41, [2.0, 10.0]), duration=0.5,
+                         kwargs=dict(dt=0.01, rtol=1e-6, atol=1e-6, save_every=0.125, output_types=_ITS)),
+    "vdp_cn_f64": dict(system=VDP, algorithm="crank_nicolson", precision="float64", inputs=("vdp", 2, 42, [2.0, 10.0]),
+                       duration=0.5, kwargs=dict(rtol=1e-6, atol=1e-6, save_every=0.125, output_types=_ITS)),
+    "vdp_trap_f32": dict(system=VDP, algorithm="trapezoidal_dirk", precision="float32",
+                         inputs=("vdp", 2, 43, [2.0, 10.0]), duration=0.5,
+                         kwargs=dict(dt=0.01, rtol=1e-6, atol=1e-6, save_every=0.125, output_types=_ITS)),
+    "vdp_sdirk22_f64": dict(system=VDP, algorithm="sdirk_2_2", precision="float64",
+                            inputs=("vdp", 2, 44, [2.0, 10.0]), duration=0.5,
+                            kwargs=dict(dt=0.01, rtol=1e-7, atol=1e-7, save_every=0.125, output_types=_ITS)),
+    "vdp_midpoint_f64": dict(system=VDP, algorithm="implicit_midpoint", precision="float64",
+                             inputs=("vdp", 2, 45, [2.0, 10.0]), duration=0.5,
+                             kwargs=dict(dt=0.01, rtol=1e-7, atol=1e-7, save_every=0.125, output_types=_ITS)),
+    "vdp_kvaerno3_f64": dict(system=VDP, algorithm="kvaerno3", precision="float64",
+                             inputs=("vdp", 2, 46, [2.0, 10.0]), duration=0.5,
+                             kwargs=dict(rtol=1e-7, atol=1e-7, save_every=0.125, output_types=_ITS)),
+    "vdp_kvaerno5_f32": dict(system=VDP, algorithm="kvaerno5", precision="float32",
+                             inputs=("vdp", 2, 47, [2.0, 10.0]), duration=0.5,
+                             kwargs=dict(rtol=1e-6, atol=1e-6, save_every=0.125, output_types=_ITS)),
+    "vdp_gl2_f32": dict(system=VDP, algorithm="firk_gauss_legendre_2", precision="float32",
+                        inputs=("vdp", 2, 48, [2.0, 10.0]), duration=0.5,
+                        kwargs=dict(dt=0.02, rtol=1e-6, atol=1e-6, save_every=0.125, output_types=_ITS)),
+    "vdp_gl4_f64": dict(system=VDP, algorithm="firk_gauss_legendre_4", precision="float64",
+                        inputs=("vdp", 2, 49, [2.0, 10.0]), duration=0.5,
+                        kwargs=dict(dt=0.025, rtol=1e-8, atol=1e-8, save_every=0.125, output_types=_ITS)),
+    "vdp_rodas3p_f64": dict(system=VDP, algorithm="rodas3p", precision="float64",
+                            inputs=("vdp", 4, 50, [1.0, 3.0, 10.0, 30.0]), duration=1.0,
+                            kwargs=dict(rtol=1e-7, atol=1e-7, save_every=0.25, output_types=_ITS)),
+    "vdp_rosenbrock23_f32": dict(system=VDP, algorithm="rosenbrock23", precision="float32",
+                                 inputs=("vdp", 4, 51, [1.0, 3.0, 10.0, 30.0]), duration=1.0,
+                                 kwargs=dict(rtol=1e-5, atol=1e-5, save_every=0.25, output_types=_ITS)),
+})
+
 
 def case_inputs(case):
     kind = case["inputs"][0]

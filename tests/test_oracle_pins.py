@@ -4,9 +4,13 @@ The fixtures ``tests/golden/ref_*.npz`` were produced by running the
 unmodified reference kernels on the CPU (Numba CUDA simulator) through
 ``tests/golden/make_reference_fixtures.py``.  In float64 the oracle must
 reproduce them to a small fraction of the tolerance envelope with the same
-step and rejection counts; in float32 the reference compiles with fast-math
-(approximate division and transcendentals), so rounding paths differ and
-agreement is judged in tolerance units on non-chaotic cases.
+step and rejection counts.  In float32 the oracle's own arithmetic order
+differs from the reference's (it forms the Jacobian as a matrix and applies
+it with one contraction, where the reference evaluates generated ``J v``
+expressions; its system expressions are SymPy lambdas), so rounding paths
+part and agreement is judged in tolerance units on non-chaotic cases.  The
+bit-level comparison with the reference is the generated device code's
+(``test_emulated_parity.py``).
 """
 
 import json
