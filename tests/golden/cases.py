@@ -186,7 +186,7 @@ CASES.update({
                              kwargs=dict(rtol=1e-7, atol=1e-7, save_every=0.125, output_types=_ITS)),
     "vdp_kvaerno5_f32": dict(system=VDP, algorithm="kvaerno5", precision="float32",
                              inputs=("vdp", 2, 47, [2.0, 10.0]), duration=0.5,
-                             kwargs=dict(rtol=1e-6, atol=1e-6, save_every=0.125, output_types=_ITS)),
+                             kwargs=dict(rtol=1e-5, atol=1e-5, save_every=0.125, output_types=_ITS)),
     "vdp_gl2_f32": dict(system=VDP, algorithm="firk_gauss_legendre_2", precision="float32",
                         inputs=("vdp", 2, 48, [2.0, 10.0]), duration=0.5,
                         kwargs=dict(dt=0.02, rtol=1e-6, atol=1e-6, save_every=0.125, output_types=_ITS)),
