@@ -44,7 +44,7 @@ VDP = ["dx = y", "dy = mu * (1 - x**2) * y - x"]
 RTOL = ATOL = 1e-6
 SOLVED_TOL_UNITS = 10.0
 SEED = 2
-NEW = dict(algorithm="ros3p", rtol=RTOL, atol=ATOL, linear_correction_type="gmres", preconditioner_type=None,
+NEW = dict(algorithm="ros3p", rtol=RTOL, atol=ATOL, linear_correction_type="direct", preconditioner_type=None,
            mixed_precision=True, kernel="persistent")
 NEW_RADAU = dict(NEW, algorithm="radau")
 PLAIN = dict(algorithm="ros3p", rtol=RTOL, atol=ATOL, kernel="plain", max_steps=1_000_000)
@@ -349,7 +349,7 @@ def hetero_arm(args, dev):
     rob = create_ODE_system(ROBERTSON, states={"y1": 1.0, "y2": 0.0, "y3": 0.0},
                             parameters={"k1": 0.04, "k2": 3e7, "k3": 1e4}, precision=f32)
     common = dict(rtol=1e-4, output_types=["state"], mixed_precision=True, device=dev.index)
-    gm = dict(linear_correction_type="gmres", preconditioner_type=None)
+    gm = dict(linear_correction_type=args.linear, preconditioner_type=None)
     solvers = [Solver(lor, algorithm="dormand-prince-54", atol=1e-8, **common),
                Solver(vdp, algorithm="ros3p", atol=1e-8, **gm, **common),
                Solver(rob, algorithm="ros3p", atol=1e-10, **gm, **common)]
@@ -673,7 +673,10 @@ def gpu_arm(args, rank: int, world: int, dist):
             "dtype": "f32 stepping, f64 time/control/norms",
             "data": "synthetic (seeded)",
             "config": {"workload": WORKLOAD, "n_systems_per_gpu": n, "algorithm": "ros3p",
-                       "linear_solver": "gmres (unpreconditioned)", "kernel": "persistent work-stealing",
+                       "linear_solver": {"gmres": "gmres (unpreconditioned)",
+                                         "direct": "dense LU in registers, one factorisation per step"}.get(
+                                             args.linear, args.linear),
+                       "kernel": "persistent work-stealing",
                        "precision": "mixed", "solved_if": f"status==0 and error<={SOLVED_TOL_UNITS} tol units",
                        "truth": f"FP64 Radau IIA5 rtol=atol=1e-10 on {T} seeded runs",
                        "l2": "flushed (256 MB write) before every timed launch",
@@ -746,6 +749,8 @@ def main():
     ap.add_argument("--cpu-per-core", type=int, default=2)
     ap.add_argument("--cpu-max-steps", type=int, default=3000)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--linear", default="direct", choices=["gmres", "direct", "minimal_residual", "bicgstab"],
+                    help="linear solver of the engine's implicit legs (headline, Radau, mixed batch)")
     ap.add_argument("--adj-n", type=int, default=262144, help="FitzHugh-Nagumo adjoint leg size (0: skip)")
     ap.add_argument("--lorenz-n", type=int, default=4096, help="Lorenz saved-trajectory leg size (0: skip)")
     ap.add_argument("--c5-n", type=int, default=1 << 20, help="heterogeneous three-system leg size (0: skip)")
@@ -755,6 +760,8 @@ def main():
     ap.add_argument("--adj-steps", type=int, default=3)
     ap.add_argument("--adj-warmup", type=int, default=1)
     args = ap.parse_args()
+    for cfg in (NEW, NEW_RADAU):
+        cfg["linear_correction_type"] = args.linear
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if args.impl == "reference":

@@ -343,6 +343,7 @@ def generate_system(system: SymbolicODE, struct_name: str = "System", second_ord
            f"    static constexpr int ND = {system.num_drivers};",
            f"    static constexpr int NO = {system.num_observables};",
            f"    static constexpr int NJ = {max(nnz, 1)};",
+           f"    static constexpr bool HAS_DFDT = {str(any(e != 0 for e in dfdt)).lower()};",
            f"    static constexpr int NPJ = {max(len(pjac_pattern), 1)};",
            fn("dxdt(const R* __restrict__ y, const R* __restrict__ p, const R* __restrict__ d, R t, R* __restrict__ f)",
               f"        {unused}\n" + body_f),
@@ -381,6 +382,7 @@ def system_stub(system: SymbolicODE, struct_name: str = "System") -> GeneratedSy
                      f"    static constexpr int ND = {system.num_drivers};",
                      f"    static constexpr int NO = {system.num_observables};",
                      "    static constexpr int NJ = 1;",
+                     "    static constexpr bool HAS_DFDT = true;",
                      "    static constexpr int NPJ = 1;",
                      "};"])
     return GeneratedSystem(name=system.name, source=src, n=n, n_params=system.num_parameters,

@@ -23,7 +23,7 @@ enum Status : int {
 
 // Algorithm families and linear solvers selected by the configuration.
 enum Algo : int { ALGO_ERK = 0, ALGO_DIRK = 1, ALGO_FIRK = 2, ALGO_ROSENBROCK = 3 };
-enum Lin : int { LIN_MR = 0, LIN_SD = 1, LIN_BICGSTAB = 2, LIN_GMRES = 3 };
+enum Lin : int { LIN_MR = 0, LIN_SD = 1, LIN_BICGSTAB = 2, LIN_GMRES = 3, LIN_DIRECT = 4 };
 enum Ctrl : int { CTRL_FIXED = 0, CTRL_I = 1, CTRL_PI = 2, CTRL_PID = 3, CTRL_GUSTAFSSON = 4 };
 
 // Python's max/min semantics for two arguments (the reference uses the

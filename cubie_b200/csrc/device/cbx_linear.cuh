@@ -383,4 +383,111 @@ __device__ __forceinline__ int solve_gmres(const Op& op, typename Cfg::R* rhs,
     return converged ? SUCCESS : MAX_LINEAR_ITERATIONS_EXCEEDED;
 }
 
+// Dense LU with partial pivoting, held in registers, for operators small
+// enough to form (one system per thread, K <= a few dozen).  The matrix is
+// built column by column from K operator applications, so it is exactly
+// the operator the Krylov solvers see.  Row interchanges are done with
+// compile-time-indexed selects (no runtime register indexing), and the
+// inverse diagonal is kept so a solve costs K^2 multiply-adds.  A
+// Rosenbrock step factors once and solves every stage with the factors,
+// which is the reason W/Rosenbrock methods freeze their Jacobian.
+template <class R, int K>
+struct DenseLU {
+    R m[K][K];
+    R rdiag[K];
+    int piv[K];
+    bool ok;
+    template <class Op>
+    __device__ __forceinline__ void factor(const Op& op) {
+#pragma unroll
+        for (int j = 0; j < K; ++j) {
+            R e[K], col[K];
+#pragma unroll
+            for (int i = 0; i < K; ++i) e[i] = (i == j) ? R(1) : R(0);
+            op.apply(e, col);
+#pragma unroll
+            for (int i = 0; i < K; ++i) m[i][j] = col[i];
+        }
+        ok = true;
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            int p = k;
+            R best = absv(m[k][k]);
+#pragma unroll
+            for (int i = k + 1; i < K; ++i) {
+                const R a = absv(m[i][k]);
+                if (a > best) {
+                    best = a;
+                    p = i;
+                }
+            }
+            piv[k] = p;
+            ok = ok && (best > R(0)) && is_finite(best);
+#pragma unroll
+            for (int i = k + 1; i < K; ++i) {
+                const bool sw = (i == p);
+#pragma unroll
+                for (int c = 0; c < K; ++c) {
+                    const R t = m[k][c];
+                    m[k][c] = sw ? m[i][c] : t;
+                    m[i][c] = sw ? t : m[i][c];
+                }
+            }
+            const R inv = R(1) / m[k][k];
+            rdiag[k] = inv;
+#pragma unroll
+            for (int i = k + 1; i < K; ++i) {
+                const R l = m[i][k] * inv;
+                m[i][k] = l;
+#pragma unroll
+                for (int c = k + 1; c < K; ++c) m[i][c] -= l * m[k][c];
+            }
+        }
+    }
+    // x = A^-1 b (b is left untouched).
+    __device__ __forceinline__ void solve(const R* b, R* x) const {
+        R y[K];
+#pragma unroll
+        for (int i = 0; i < K; ++i) y[i] = b[i];
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+#pragma unroll
+            for (int i = k + 1; i < K; ++i) {
+                const bool sw = (i == piv[k]);
+                const R t = y[k];
+                y[k] = sw ? y[i] : t;
+                y[i] = sw ? t : y[i];
+            }
+        }
+#pragma unroll
+        for (int i = 1; i < K; ++i)
+#pragma unroll
+            for (int c = 0; c < i; ++c) y[i] -= m[i][c] * y[c];
+#pragma unroll
+        for (int i = K - 1; i >= 0; --i) {
+#pragma unroll
+            for (int c = i + 1; c < K; ++c) y[i] -= m[i][c] * y[c];
+            y[i] *= rdiag[i];
+        }
+#pragma unroll
+        for (int i = 0; i < K; ++i) x[i] = y[i];
+    }
+};
+
+// The direct solve behind ``linear_solve`` for Newton iterations (the
+// operator changes with every iterate, so it is formed and factored per
+// call).  ``rhs`` holds b on entry and is left as the (zero) residual;
+// ``iters`` is 1.
+template <class Cfg, class Op>
+__device__ __forceinline__ int solve_direct(const Op& op, typename Cfg::R* rhs, typename Cfg::R* x, int& iters) {
+    using R = typename Cfg::R;
+    DenseLU<R, Op::K> lu;
+    lu.factor(op);
+    lu.solve(rhs, x);
+#pragma unroll
+    for (int i = 0; i < Op::K; ++i) rhs[i] = R(0);
+    iters = 1;
+    return lu.ok ? SUCCESS : MAX_LINEAR_ITERATIONS_EXCEEDED;
+}
+
 }  // namespace cbx

@@ -36,6 +36,8 @@ __device__ __forceinline__ int linear_solve(const Op& op, typename Cfg::R* rhs, 
         return solve_bicgstab<Cfg, Op>(op, rhs, x, iters);
     } else if constexpr (Cfg::LIN == LIN_GMRES) {
         return solve_gmres<Cfg, Op>(op, rhs, x, iters);
+    } else if constexpr (Cfg::LIN == LIN_DIRECT) {
+        return solve_direct<Cfg, Op>(op, rhs, x, iters);
     } else {
         return solve_mr<Cfg, Op, Cfg::LIN == LIN_SD>(op, rhs, x, iters);
     }

@@ -207,11 +207,15 @@ struct RosenbrockStep {
         const R inv_dt = R(1) / dt;
         R J[Sys::NJ];
         Sys::template jac<R>(y, ctx.p, drv, t, J);
-        R dd[ND > 0 ? ND : 1];
-        if constexpr (ND > 0) Drivers<Cfg>::deriv(t, ctx.coeffs, dd);
-        else dd[0] = R(0);
+        // h times the time derivative of f (explicit t and driver chain
+        // rule); skipped for systems where it is identically zero
         R tdv[N];
-        Sys::template dfdt<R>(y, ctx.p, drv, dd, t, tdv);
+        if constexpr (Sys::HAS_DFDT) {
+            R dd[ND > 0 ? ND : 1];
+            if constexpr (ND > 0) Drivers<Cfg>::deriv(t, ctx.coeffs, dd);
+            else dd[0] = R(0);
+            Sys::template dfdt<R>(y, ctx.p, drv, dd, t, tdv);
+        }
         // The proposed state starts from y and takes each stage's weighted
         // increment in turn (or is the stage state whose row of a equals b);
         // the error likewise, in the reference's order of operations.
@@ -219,7 +223,7 @@ struct RosenbrockStep {
         // update of the mixed-precision mode.
 #pragma unroll
         for (int i = 0; i < N; ++i) {
-            tdv[i] *= dt;
+            if constexpr (Sys::HAS_DFDT) tdv[i] *= dt;
             delta[i] = R(0);
             ynew[i] = y[i];
             if (Tab::HAS_ERR) err[i] = R(0);
@@ -229,6 +233,12 @@ struct RosenbrockStep {
         R drv_stage[ND > 0 ? ND : 1];
         int status = SUCCESS;
         SingleStageOp<Cfg> op{J, gamma * dt, y, ctx.tol_scale};
+        // direct solves: one factorisation of I - gamma h J serves every stage
+        DenseLU<R, N> lu;
+        if constexpr (Cfg::LIN == LIN_DIRECT) {
+            lu.factor(op);
+            if (!lu.ok) status |= MAX_LINEAR_ITERATIONS_EXCEEDED;
+        }
         // One loop over the stages with a single call site of the linear
         // solver keeps one copy of it in the instruction stream.  The stage
         // index is a run-time value here, so tableau entries and the stored
@@ -236,8 +246,11 @@ struct RosenbrockStep {
         // (the increments stay in registers).  The initial guess of every
         // stage is the solution of the one before it (the first stage uses
         // the previous step's last increment), which is what ``ps.guess``
-        // already holds when the solve starts.
-#pragma unroll 1
+        // already holds when the solve starts.  With direct solves the
+        // solve is a few multiply-adds, so the loop is unrolled and every
+        // select folds to a constant.
+        constexpr int STAGE_UNROLL = (Cfg::LIN == LIN_DIRECT) ? S : 1;
+#pragma unroll (STAGE_UNROLL)
         for (int stage = 0; stage < S; ++stage) {
             R c_s = R(0), gs_s = R(0), b_s = R(0), d_s = R(0);
 #pragma unroll
@@ -285,11 +298,17 @@ struct RosenbrockStep {
             Sys::template dxdt<R>(Y, ctx.p, ND > 0 ? drv_stage : drv, stage_time, f);
 #pragma unroll
             for (int i = 0; i < N; ++i) {
-                const R rv = (stage > 0) ? f[i] + rhs[i] * inv_dt + gs_s * tdv[i] : f[i] + gs_s * tdv[i];
+                R rv = (stage > 0) ? f[i] + rhs[i] * inv_dt : f[i];
+                if constexpr (Sys::HAS_DFDT) rv = rv + gs_s * tdv[i];
                 rhs[i] = rv * dt * gamma;
             }
             int it = 0;
-            status |= linear_solve<Cfg>(op, rhs, ps.guess, it);
+            if constexpr (Cfg::LIN == LIN_DIRECT) {
+                lu.solve(rhs, ps.guess);
+                it = 1;
+            } else {
+                status |= linear_solve<Cfg>(op, rhs, ps.guess, it);
+            }
             its.kit_all += it;
 #pragma unroll
             for (int i = 0; i < N; ++i) {

@@ -550,18 +550,21 @@ __device__ __forceinline__ bool warp_iterate(WarpLane<Cfg>& L, WarpCtx<Cfg>& w, 
     L.irrecoverable = L.irrecoverable || (!Cfg::ADAPTIVE && step_failed);
     bool accept;
     if constexpr (Cfg::ADAPTIVE) {
-        // error norm over the warp (Controller::error_norm2)
-        C nrm2 = C(0);
+        // error norm over the warp (Controller::error_norm2), in the gain
+        // precision G
+        using G = typename Cfg::G;
+        G nrm2 = G(0);
+        const G ts = G(w.tol_scale);
 #pragma unroll
         for (int i = 0; i < NL; ++i) {
             if (!w.valid(i)) continue;
             const int c = w.lane + 32 * i;
-            const C e = step_failed ? C(1e16) : pymax(C(absv(err[i])), C(1e-16));
-            const C tol = C(Cfg::atol(c)) + C(Cfg::rtol(c)) * w.tol_scale * pymax(C(absv(ynew[i])), C(absv(L.y[i])));
-            const C ratio = e / tol;
+            const G e = step_failed ? G(1e16) : pymax(G(absv(err[i])), G(1e-16));
+            const G tol = G(Cfg::atol(c)) + G(Cfg::rtol(c)) * ts * pymax(G(absv(ynew[i])), G(absv(L.y[i])));
+            const G ratio = e / tol;
             nrm2 += ratio * ratio;
         }
-        nrm2 = warp_sum(nrm2) * C(Cfg::CTL_INV_N);
+        nrm2 = warp_sum(nrm2) * G(Cfg::CTL_INV_N);
         bool ctl_accept = false;
         const int ctl_status = Controller<Cfg>::update_with_norm(L.dt, nrm2, nit, truncated, ctl_accept, L.ctl);
         accept = ctl_accept && !step_failed;

@@ -31,7 +31,7 @@ ALGO_IDS = {ERK: "cbx::ALGO_ERK", DIRK: "cbx::ALGO_DIRK", FIRK: "cbx::ALGO_FIRK"
 STEP_TYPES = {ERK: "cbx::ErkStep<Cfg>", DIRK: "cbx::DirkStep<Cfg>", FIRK: "cbx::FirkStep<Cfg>",
               ROSENBROCK: "cbx::RosenbrockStep<Cfg>"}
 LIN_IDS = {"minimal_residual": "cbx::LIN_MR", "steepest_descent": "cbx::LIN_SD",
-           "bicgstab": "cbx::LIN_BICGSTAB", "gmres": "cbx::LIN_GMRES"}
+           "bicgstab": "cbx::LIN_BICGSTAB", "gmres": "cbx::LIN_GMRES", "direct": "cbx::LIN_DIRECT"}
 ADJOINT_FAMILIES = {ERK, ROSENBROCK}
 CTRL_IDS = {"fixed": "cbx::CTRL_FIXED", "i": "cbx::CTRL_I", "pi": "cbx::CTRL_PI",
             "pid": "cbx::CTRL_PID", "gustafsson": "cbx::CTRL_GUSTAFSSON"}
@@ -272,6 +272,7 @@ def family_block(system: SymbolicODE, spec: KernelSpec, gen: GeneratedSystem, ns
         f"    using Sys = {ns}::System;",
         f"    using R = {rtype};",
         f"    using C = {ctype};",
+        f"    using G = {'float' if spec.mixed_precision else ctype};",
         f"    using Tab = {ns}::Tab;",
         f"    using Summ = {ns}::Summ;",
         f"    using Idx = {ns}::Idx;",

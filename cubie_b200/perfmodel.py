@@ -18,6 +18,10 @@ multiply or divide on each element:
   update (2 K per basis vector + 7 K);
 * MR/SD iteration: preconditioner (order m applications), one application,
   two dot products (4 K), two axpys (4 K), one weighted norm;
+* direct solve (dense LU with partial pivoting): forming the operator
+  from K applications, factoring (sum over pivots of one reciprocal and
+  2 (K-k-1)^2 + (K-k-1) for the eliminations), and 2 K^2 per solve; a
+  Rosenbrock step factors once and solves every stage;
 * the step-size controller: 9 N plus two powers.
 
 The result is the work the method performs, not the instruction count the
@@ -36,8 +40,15 @@ def _f(flops: Dict[str, FlopCount], name: str) -> int:
     return flops[name].flops if name in flops else 0
 
 
+def direct_factor_flops(K: int, op_flops: int) -> float:
+    elim = sum(1 + 2 * (K - k - 1) ** 2 + (K - k - 1) for k in range(K))
+    return K * op_flops + elim
+
+
 def linear_iteration_flops(lin: str, K: int, op_flops: int, precond_order: int, preconditioned: bool,
                            restart: int) -> float:
+    if lin == "direct":
+        return 2 * K * K
     if lin == "gmres":
         m = min(restart, K)
         j_avg = (m - 1) / 2.0
@@ -50,6 +61,8 @@ def linear_iteration_flops(lin: str, K: int, op_flops: int, precond_order: int, 
 
 
 def linear_solve_overhead(lin: str, K: int, op_flops: int, restart: int) -> float:
+    if lin == "direct":
+        return direct_factor_flops(K, op_flops)
     if lin == "gmres":
         m = min(restart, K)
         return 2 * 7 * K + op_flops + K + 2 * K * m + 7 * K + m * m
@@ -79,6 +92,8 @@ def estimate_flops(spec, gen, totals: Dict[str, int]) -> float:
         per_step = jac + dfdt + n + S * rhs + S * 12 * n + 4 * n * S + n
         solves = steps * S
         it = linear_iteration_flops(lin, K, op, spec.preconditioner_order, spec.preconditioned, spec.gmres_restart)
+        if lin == "direct":
+            return steps * (per_step + ctrl + comp + direct_factor_flops(K, op)) + krylov * it
         return steps * (per_step + ctrl + comp) + solves * linear_solve_overhead(lin, K, op, spec.gmres_restart) \
             + krylov * it
     if tab.kind == FIRK:

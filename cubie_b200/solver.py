@@ -52,6 +52,9 @@ OUTPUT_KEYS = {"output_types", "saved_state_indices", "saved_observable_indices"
                "summarised_state_indices", "summarised_observable_indices",
                "save_variables", "summarise_variables"}
 LOOP_KEYS = {"save_every", "summarise_every", "sample_summaries_every"}
+# largest operator (states, or stages x states for fully implicit tableaus)
+# the register-resident dense LU forms
+DIRECT_MAX_WIDTH = 16
 EXECUTION_KEYS = {"mixed_precision", "kernel", "block_size", "min_blocks_per_sm", "max_steps", "device", "fast_math",
                   "precision", "adjoint", "layout"}
 IGNORED_KEYS = {"memory_settings", "cache", "auto_memory", "lineinfo", "time_logging_level",
@@ -220,9 +223,17 @@ class Solver:
         tab = self.tableau
         eps = float(np.finfo(self.precision).eps)
         lin = user.get("linear_correction_type", "minimal_residual")
-        if lin not in ("steepest_descent", "minimal_residual", "bicgstab", "gmres"):
+        if lin not in ("steepest_descent", "minimal_residual", "bicgstab", "gmres", "direct"):
             raise ValueError("linear_correction_type must be one of 'steepest_descent', "
-                             f"'minimal_residual', 'bicgstab', 'gmres'; got '{lin}'.")
+                             f"'minimal_residual', 'bicgstab', 'gmres', 'direct'; got '{lin}'.")
+        if lin == "direct":
+            # dense LU in registers: one system per thread, small operators
+            width = n * (tab.stage_count if tab.kind == "firk" else 1)
+            if self.layout != "thread":
+                raise ValueError("linear_correction_type='direct' needs layout='thread'")
+            if width > DIRECT_MAX_WIDTH:
+                raise ValueError(f"linear_correction_type='direct' forms the {width}x{width} operator; "
+                                 f"at most {DIRECT_MAX_WIDTH} is supported")
         self.linear_correction_type = lin
         implicit = tab.kind != "erk"
         # inner tolerances derived from the controller unless given

@@ -99,3 +99,22 @@ def test_mixed_precision_error_matches_float64(cuda_device, name):
     err64 = tol_units(f64.state[:k, :-1], truth[:k], 1e-6, 1e-6)
     errmx = tol_units(mixed.state[:k, :-1], truth[:k], 1e-6, 1e-6)
     assert errmx <= max(2.0 * err64, 1.0), (errmx, err64)
+
+
+DIRECT_CASES = ["vdp_ros3p_f32", "vdp_ros3p_bicgstab_f64", "vdp_rodas3p_f64", "vdp_radau_f64", "vdp_sdirk4_f64",
+                "vdp_kvaerno3_f64", "vdp_gl4_f64", "driven_ros3p_clamped_f64"]
+
+
+@pytest.mark.parametrize("name", DIRECT_CASES)
+def test_direct_solver_matches_oracle(cuda_device, name):
+    """``linear_correction_type='direct'`` (register LU) against the oracle's
+    exact dense solve: same status words and step/rejection counts in
+    float64, trajectories within the usual bars."""
+    case, atol, rtol, bar = _bars(name)
+    out = run_oracle(case, linear_correction_type="direct")
+    res = _solve(case, kernel="persistent", linear_correction_type="direct",
+                 output_types=["state", "time", "iteration_counters"])
+    assert res.status_codes.tolist() == out["status"].tolist()
+    assert tol_units(res.state, out["state"], atol, rtol) < bar
+    if case["precision"] == "float64":
+        np.testing.assert_array_equal(res.iteration_counters[:, 2:, :], out["iteration_counters"][:, 2:, :])
