@@ -554,12 +554,13 @@ def gpu_arm(args, rank: int, world: int, dist):
         totals = None
         for it in range(warmup + steps):
             bufs["totals"].zero_()
-            args_ = solver.make_args(prep, bufs, inits_t, params_t, None, n_runs, float(durs[:n_runs].max()),
-                                     0.0, 0.0, dur_t, None)
             _native.flush_l2(flush.data_ptr(), flush.numel() * 4, stream.cuda_stream)
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(stream)
+            # the claim order (runs by decreasing horizon) is part of the step
+            args_ = solver.make_args(prep, bufs, inits_t, params_t, None, n_runs, float(durs[:n_runs].max()),
+                                     0.0, 0.0, dur_t, None, order_t=solver.run_order(dur_t))
             prep["module"].launch(args_, kernel, solver.block_size, 0, stream.cuda_stream)
             e1.record(stream)
             e1.synchronize()
@@ -676,7 +677,7 @@ def gpu_arm(args, rank: int, world: int, dist):
                        "linear_solver": {"gmres": "gmres (unpreconditioned)",
                                          "direct": "dense LU in registers, one factorisation per step"}.get(
                                              args.linear, args.linear),
-                       "kernel": "persistent work-stealing",
+                       "kernel": "persistent work-stealing, runs claimed longest horizon first",
                        "precision": "mixed", "solved_if": f"status==0 and error<={SOLVED_TOL_UNITS} tol units",
                        "truth": f"FP64 Radau IIA5 rtol=atol=1e-10 on {T} seeded runs",
                        "l2": "flushed (256 MB write) before every timed launch",
@@ -758,7 +759,7 @@ def main():
     ap.add_argument("--c3-n", type=int, default=65536, help="Hodgkin-Huxley cable leg size (0: skip)")
     ap.add_argument("--c3-steps", type=int, default=2)
     ap.add_argument("--adj-steps", type=int, default=3)
-    ap.add_argument("--adj-warmup", type=int, default=1)
+    ap.add_argument("--adj-warmup", type=int, default=3)
     args = ap.parse_args()
     for cfg in (NEW, NEW_RADAU):
         cfg["linear_correction_type"] = args.linear

@@ -46,6 +46,7 @@ class SolveArgs(ctypes.Structure):
         ("work_counter", ctypes.c_void_p),
         ("totals", ctypes.c_void_p),
         ("abort_flag", ctypes.c_void_p),
+        ("run_order", ctypes.c_void_p),
         ("n_runs", ctypes.c_longlong),
         ("run_stride", ctypes.c_longlong),
         ("max_steps", ctypes.c_longlong),

@@ -32,6 +32,9 @@ typedef struct cbx_solve_args {
     unsigned long long* work_counter; /* persistent launch: next run to claim */
     unsigned long long* totals;       /* [4]: steps, rejections, newton, krylov */
     const volatile int* abort_flag;   /* host-visible abort request, or NULL */
+    const long long* run_order; /* persistent launch: claim k integrates run
+                                   run_order[k] (NULL: run k); a permutation
+                                   of [0, n_runs) */
     /* sizes */
     long long n_runs;
     long long run_stride;

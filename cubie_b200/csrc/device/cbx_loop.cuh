@@ -412,7 +412,10 @@ __device__ __forceinline__ long long claim_run(unsigned long long* counter) {
 
 // Persistent work-stealing kernel: resident warps loop until the run
 // counter is exhausted; a lane whose run finishes claims a new one at the
-// top of the next iteration.  blockDim.x must be a multiple of 32.
+// top of the next iteration.  Claims follow ``run_order`` when given (the
+// host orders runs longest first, so the last claims are the short runs
+// and warps do not idle behind a few long ones at the end).  blockDim.x
+// must be a multiple of 32.
 template <class Cfg>
 __device__ __forceinline__ void run_persistent(const cbx_solve_args a) {
     __shared__ BlockTotals bt;
@@ -421,9 +424,9 @@ __device__ __forceinline__ void run_persistent(const cbx_solve_args a) {
     bool active = false, exhausted = false;
     while (true) {
         if (!active && !exhausted) {
-            const long long run = claim_run(a.work_counter);
-            if (run < a.n_runs) {
-                lane_begin<Cfg>(L, a, run);
+            const long long k = claim_run(a.work_counter);
+            if (k < a.n_runs) {
+                lane_begin<Cfg>(L, a, a.run_order ? a.run_order[k] : k);
                 active = true;
             } else {
                 exhausted = true;

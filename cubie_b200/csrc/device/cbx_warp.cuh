@@ -653,7 +653,7 @@ __device__ __forceinline__ void run_warp(const cbx_solve_args& a) {
         r = __shfl_sync(kWarpFull, r, 0);
         if ((long long)r >= a.n_runs) break;
         WarpLane<Cfg> L;
-        warp_begin<Cfg>(L, w, a, (long long)r);
+        warp_begin<Cfg>(L, w, a, a.run_order ? a.run_order[r] : (long long)r);
         while (!warp_iterate<Cfg>(L, w, a)) {
         }
         if (lane == 0) {

@@ -56,7 +56,7 @@ LOOP_KEYS = {"save_every", "summarise_every", "sample_summaries_every"}
 # the register-resident dense LU forms
 DIRECT_MAX_WIDTH = 16
 EXECUTION_KEYS = {"mixed_precision", "kernel", "block_size", "min_blocks_per_sm", "max_steps", "device", "fast_math",
-                  "precision", "adjoint", "layout"}
+                  "precision", "adjoint", "layout", "schedule"}
 IGNORED_KEYS = {"memory_settings", "cache", "auto_memory", "lineinfo", "time_logging_level",
                 "profileCUDA", "cache_settings"}
 RENAMED = {"dt_save": "save_every", "dt_summarise": "summarise_every",
@@ -145,6 +145,11 @@ class Solver:
         if layout not in ("thread", "warp"):
             raise ValueError("layout must be 'thread', 'warp' or 'auto'")
         self.layout = layout
+        # claim order of persistent launches: "auto" / "longest_first" sort
+        # runs by decreasing per-run horizon when horizons are given
+        self.schedule = str(execution.get("schedule", "auto"))
+        if self.schedule not in ("auto", "longest_first", "index"):
+            raise ValueError("schedule must be 'auto', 'longest_first' or 'index'")
         self.max_steps = int(execution.get("max_steps", 0))
         self.device = int(execution.get("device", 0))
         self.fast_math = bool(execution.get("fast_math", True))
@@ -573,8 +578,9 @@ class Solver:
         coeff_t = None
         if interp is not None:
             coeff_t = torch.as_tensor(interp.coefficients.astype(self.precision), device=dev).contiguous()
+        order_t = self.run_order(dur_t)
         args = self.make_args(prep, bufs, inits_t, params_t, coeff_t, n_runs, duration, settling_time, t0,
-                              dur_t, tol_t)
+                              dur_t, tol_t, order_t=order_t)
         kernel = self.launch_kind
         s = stream if stream is not None else torch.cuda.current_stream(dev)
         e0 = torch.cuda.Event(enable_timing=True)
@@ -620,8 +626,19 @@ class Solver:
         }
         return bufs
 
+    def run_order(self, dur_t):
+        """Claim order of a persistent launch: with per-run horizons and
+        ``schedule='longest_first'`` (the default ``'auto'`` when horizons
+        are given), the runs sorted by decreasing horizon, as a device
+        int64 permutation; otherwise None (claim in index order).  Each
+        run's result does not depend on the order."""
+        if dur_t is None or self.schedule == "index" or self.launch_kind == 0:
+            return None
+        torch = _torch()
+        return torch.argsort(dur_t, descending=True).to(torch.int64).contiguous()
+
     def make_args(self, prep, bufs, inits_t, params_t, coeff_t, n_runs, duration, settling_time, t0,
-                  dur_t=None, tol_t=None, max_steps=None) -> "_native.SolveArgs":
+                  dur_t=None, tol_t=None, max_steps=None, order_t=None) -> "_native.SolveArgs":
         def ptr(t):
             return t.data_ptr() if t is not None else None
         a = _native.SolveArgs()
@@ -640,6 +657,7 @@ class Solver:
         a.work_counter = ptr(bufs["work"])
         a.totals = ptr(bufs["totals"])
         a.abort_flag = None
+        a.run_order = ptr(order_t)
         a.n_runs = n_runs
         a.run_stride = n_runs
         a.max_steps = int(self.max_steps if max_steps is None else max_steps)

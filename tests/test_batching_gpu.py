@@ -59,3 +59,27 @@ def test_autotuned_solver_matches_default(cuda_device, tmp_path, monkeypatch):
     assert r.status_codes.tolist() == ref.status_codes.tolist()
     err = np.abs(r.state - ref.state) / (1e-6 + 1e-6 * np.abs(ref.state))
     assert float(np.max(err)) < 1e-3
+
+
+@pytest.mark.parametrize("lin", ["gmres", "direct"])
+def test_longest_first_claims_leave_results_unchanged(cuda_device, lin):
+    """Claiming runs by decreasing horizon (``schedule='auto'`` with per-run
+    durations) changes only which lane integrates which run: every run's
+    saved state, status and the launch totals equal the index-order ones
+    bit for bit."""
+    rng = np.random.default_rng(7)
+    n = 5000
+    mu = 10.0 ** rng.uniform(0, 2.5, n)
+    x0 = rng.uniform(-2, 2, (2, n))
+    durs = 2.0 * mu
+    out = {}
+    from cubie_b200 import Solver, create_ODE_system
+    sysm = create_ODE_system(VDP, states={"x": 2.0, "y": 0.0}, parameters={"mu": 10.0}, precision=np.float32)
+    for sched in ("index", "auto"):
+        solver = Solver(sysm, algorithm="ros3p", rtol=1e-6, atol=1e-6, linear_correction_type=lin,
+                        preconditioner_type=None, mixed_precision=True, output_types=["state"], schedule=sched)
+        out[sched] = solver.solve(x0, mu[None, :], duration=float(durs.max()), durations=durs,
+                                  nan_error_trajectories=False)
+    assert out["auto"].status_codes.tolist() == out["index"].status_codes.tolist()
+    np.testing.assert_array_equal(out["auto"].state, out["index"].state)
+    assert out["auto"].totals == out["index"].totals

@@ -31,7 +31,7 @@ def test_args_struct_layout_matches_header():
     import ctypes
     from cubie_b200 import _native
     # 14 pointers, 3 int64, 5 float64, 2 int32
-    assert ctypes.sizeof(_native.SolveArgs) == 14 * 8 + 3 * 8 + 5 * 8 + 2 * 4
+    assert ctypes.sizeof(_native.SolveArgs) == 15 * 8 + 3 * 8 + 5 * 8 + 2 * 4
     # 6 pointers, 1 int64, 2 int32
     assert ctypes.sizeof(_native.AdjointArgs) == 6 * 8 + 8 + 2 * 4
 
