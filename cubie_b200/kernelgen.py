@@ -264,9 +264,9 @@ def family_block(system: SymbolicODE, spec: KernelSpec, gen: GeneratedSystem, ns
                        f"{{{', '.join(str(v) for v in vv)}}}; return v[k]; }}")
     lines.append("struct Idx {\n" + "\n".join(idx_fns) + "\n};")
     lines.append(tableau_struct(tab, spec.precision, dense))
-    lines.append(summ.device_struct())
     save_every = castp(spec.save_every) if spec.save_every is not None else 0.0
     sample_every = castp(spec.sample_summaries_every) if spec.sample_summaries_every is not None else 0.0
+    lines.append(summ.device_struct(sample_every))
     cfg = [
         "struct Cfg {",
         f"    using Sys = {ns}::System;",

@@ -100,11 +100,44 @@ for (int q = 0; q < P; ++q) { o[q] = b[3 + q]; b[3 + q] = R(0); }
 b[2] = R(0);""", ("negative_peaks",)),
 }
 
+# Finite-difference derivative metrics (dxdt_*.py, d2xdt2_*.py): the buffer
+# keeps the previous sample(s) across summary windows; differences are
+# unscaled until the save divides by the sample interval (squared for the
+# second difference).  ``idx`` (the run's summary-sample counter) gates the
+# first one or two samples, which have no history.
+_D1 = "const R d = v - b[0];"
+_D2 = "const R d = v - R(2.0) * b[0] + b[1];"
+METRICS.update({
+    "dxdt_max": Metric("dxdt_max", 2, 1, "{ " + _D1 + " if (d > b[1] && idx >= 1) b[1] = d; b[0] = v; }",
+                       "o[0] = b[1] / R(DT_SAMPLE); b[1] = R(-1.0e30);", ("dxdt_max",)),
+    "dxdt_min": Metric("dxdt_min", 2, 1, "{ " + _D1 + " if (d < b[1] && idx >= 1) b[1] = d; b[0] = v; }",
+                       "o[0] = b[1] / R(DT_SAMPLE); b[1] = R(1.0e30);", ("dxdt_min",)),
+    "dxdt_extrema": Metric(
+        "dxdt_extrema", 3, 2,
+        "{ " + _D1 + " if (d > b[1] && idx >= 1) b[1] = d; if (d < b[2] && idx >= 1) b[2] = d; b[0] = v; }",
+        "o[0] = b[1] / R(DT_SAMPLE); o[1] = b[2] / R(DT_SAMPLE); b[1] = R(-1.0e30); b[2] = R(1.0e30);",
+        ("dxdt_max", "dxdt_min")),
+    "d2xdt2_max": Metric(
+        "d2xdt2_max", 3, 1, "{ " + _D2 + " if (d > b[2] && idx >= 2) b[2] = d; b[1] = b[0]; b[0] = v; }",
+        "{ const R s2 = R(DT_SAMPLE) * R(DT_SAMPLE); o[0] = b[2] / s2; b[2] = R(-1.0e30); }", ("d2xdt2_max",)),
+    "d2xdt2_min": Metric(
+        "d2xdt2_min", 3, 1, "{ " + _D2 + " if (d < b[2] && idx >= 2) b[2] = d; b[1] = b[0]; b[0] = v; }",
+        "{ const R s2 = R(DT_SAMPLE) * R(DT_SAMPLE); o[0] = b[2] / s2; b[2] = R(1.0e30); }", ("d2xdt2_min",)),
+    "d2xdt2_extrema": Metric(
+        "d2xdt2_extrema", 4, 2,
+        "{ " + _D2 + " if (d > b[2] && idx >= 2) b[2] = d; if (d < b[3] && idx >= 2) b[3] = d; "
+        "b[1] = b[0]; b[0] = v; }",
+        "{ const R s2 = R(DT_SAMPLE) * R(DT_SAMPLE); o[0] = b[2] / s2; o[1] = b[3] / s2; "
+        "b[2] = R(-1.0e30); b[3] = R(1.0e30); }", ("d2xdt2_max", "d2xdt2_min")),
+})
+
 COMBINED = [
     (frozenset(["mean", "std", "rms"]), "mean_std_rms"),
     (frozenset(["mean", "std"]), "mean_std"),
     (frozenset(["std", "rms"]), "std_rms"),
     (frozenset(["max", "min"]), "extrema"),
+    (frozenset(["dxdt_max", "dxdt_min"]), "dxdt_extrema"),
+    (frozenset(["d2xdt2_max", "d2xdt2_min"]), "d2xdt2_extrema"),
 ]
 
 
@@ -188,10 +221,14 @@ class SummaryPlan:
                 out.extend(m.legend)
         return out
 
-    def device_struct(self) -> str:
+    def device_struct(self, sample_every: float = 0.0) -> str:
+        """The generated ``Summ`` struct; ``sample_every`` (the summary
+        sample interval, already in the system precision) scales the
+        derivative metrics."""
         lines = ["struct Summ {",
                  f"    static constexpr int BUF = {max(self.buffer_per_var, 1)};",
                  f"    static constexpr int OUT = {self.output_per_var};",
+                 f"    static constexpr double DT_SAMPLE = {float(sample_every)!r};",
                  "    template <class R> static __device__ __forceinline__ void update(R v, R* buf, int idx) {",
                  "        (void)v; (void)buf; (void)idx;"]
         off = 0

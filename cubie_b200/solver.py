@@ -673,14 +673,30 @@ class Solver:
     def collect(self, prep, bufs, n_runs, duration, settling_time, t0, nan_error_trajectories=True,
                 on_device=False) -> SolveResult:
         spec: KernelSpec = prep["spec"]
-        conv = (lambda t: t) if on_device else (lambda t: t.cpu().numpy() if t is not None else None)
+        if on_device:
+            conv = lambda t: t  # noqa: E731
+        else:
+            # one batch of asynchronous copies into pinned host memory (the
+            # host caching allocator reuses the blocks across calls), then a
+            # single wait: pageable copies would be staged through a bounce
+            # buffer one output at a time
+            torch = _torch()
+            host = {}
+            for key in ("state", "obs", "state_sum", "obs_sum", "counters", "status", "totals"):
+                t = bufs.get(key)
+                if t is not None:
+                    h = torch.empty(tuple(t.shape), dtype=t.dtype, pin_memory=True)
+                    h.copy_(t, non_blocking=True)
+                    host[id(t)] = h
+            torch.cuda.current_stream(bufs["status"].device).synchronize()
+            conv = lambda t: host[id(t)].numpy() if t is not None else None  # noqa: E731
         res = SolveResult(
             state=conv(bufs["state"]), observables=conv(bufs["obs"]),
             state_summaries=conv(bufs["state_sum"]), observable_summaries=conv(bufs["obs_sum"]),
             iteration_counters=conv(bufs["counters"]), status_codes=conv(bufs["status"]),
             save_time=spec.save_time,
         )
-        tot = bufs["totals"].cpu().numpy()
+        tot = conv(bufs["totals"]) if not on_device else bufs["totals"].cpu().numpy()
         res.totals = dict(steps=int(tot[0]), rejections=int(tot[1]), newton=int(tot[2]), krylov=int(tot[3]))
         res.kernel_ms = self.last_kernel_ms
         sysm = self.system

@@ -615,7 +615,9 @@ def integrate(system: OracleSystem, algorithm: str, inits: np.ndarray, params: n
     save_state = "state" in ot
     save_time = "time" in ot
     save_counters = "iteration_counters" in ot
-    metrics = [m for m in ot if m.split("[")[0] in ("mean", "max", "min", "rms", "std", "extrema", "peaks")]
+    metrics = [m for m in ot if m.split("[")[0] in ("mean", "max", "min", "rms", "std", "extrema", "peaks",
+                                                    "dxdt_max", "dxdt_min", "dxdt_extrema", "d2xdt2_max",
+                                                    "d2xdt2_min", "d2xdt2_extrema")]
     time_domain = save_state or save_time or save_counters
     save_every = S.save_every if time_domain else None
     save_last = time_domain and save_every is None
@@ -651,12 +653,17 @@ def integrate(system: OracleSystem, algorithm: str, inits: np.ndarray, params: n
         par = int(m.split("[")[1].split("]")[0]) if "[" in m else 0
         return name, par
     mlist = [mdef(m) for m in metrics]
-    if ("max", 0) in mlist and ("min", 0) in mlist:
-        i = min(mlist.index(("max", 0)), mlist.index(("min", 0)))
-        mlist = [x for x in mlist if x not in (("max", 0), ("min", 0))]
-        mlist.insert(i, ("extrema", 0))
-    bsize = {"mean": 1, "max": 1, "min": 1, "rms": 1, "std": 3, "extrema": 2}
-    osize = {"mean": 1, "max": 1, "min": 1, "rms": 1, "std": 1, "extrema": 2}
+    # metrics.py:345-467: requested pairs collapse into combined metrics
+    for lo, hi, combo in (("max", "min", "extrema"), ("dxdt_max", "dxdt_min", "dxdt_extrema"),
+                          ("d2xdt2_max", "d2xdt2_min", "d2xdt2_extrema")):
+        if (lo, 0) in mlist and (hi, 0) in mlist:
+            i = min(mlist.index((lo, 0)), mlist.index((hi, 0)))
+            mlist = [x for x in mlist if x not in ((lo, 0), (hi, 0))]
+            mlist.insert(i, (combo, 0))
+    bsize = {"mean": 1, "max": 1, "min": 1, "rms": 1, "std": 3, "extrema": 2, "dxdt_max": 2, "dxdt_min": 2,
+             "dxdt_extrema": 3, "d2xdt2_max": 3, "d2xdt2_min": 3, "d2xdt2_extrema": 4}
+    osize = {"mean": 1, "max": 1, "min": 1, "rms": 1, "std": 1, "extrema": 2, "dxdt_max": 1, "dxdt_min": 1,
+             "dxdt_extrema": 2, "d2xdt2_max": 1, "d2xdt2_min": 1, "d2xdt2_extrema": 2}
     buf_w = sum(3 + p if nm == "peaks" else bsize[nm] for nm, p in mlist)
     out_w = sum(p if nm == "peaks" else osize[nm] for nm, p in mlist)
     sbuf = np.zeros((B, n, max(buf_w, 1)), rt)
@@ -688,6 +695,31 @@ def integrate(system: OracleSystem, algorithm: str, inits: np.ndarray, params: n
                 sv = vals - b[:, :, 0]
                 b[:, :, 1] = np.where(m2, b[:, :, 1] + sv, b[:, :, 1])
                 b[:, :, 2] = np.where(m2, b[:, :, 2] + sv * sv, b[:, :, 2])
+            elif nm.startswith("dxdt_"):
+                # dxdt_{max,min,extrema}.py: unscaled first difference,
+                # gated until one previous sample exists
+                d = vals - b[:, :, 0]
+                primed = m2 & (idx[:, None] >= 1)
+                if nm in ("dxdt_max", "dxdt_extrema"):
+                    b[:, :, 1] = np.where(primed & (d > b[:, :, 1]), d, b[:, :, 1])
+                if nm == "dxdt_min":
+                    b[:, :, 1] = np.where(primed & (d < b[:, :, 1]), d, b[:, :, 1])
+                if nm == "dxdt_extrema":
+                    b[:, :, 2] = np.where(primed & (d < b[:, :, 2]), d, b[:, :, 2])
+                b[:, :, 0] = np.where(m2, vals, b[:, :, 0])
+            elif nm.startswith("d2xdt2_"):
+                # d2xdt2_{max,min,extrema}.py: unscaled second difference,
+                # gated until two previous samples exist
+                d = vals - rt(2.0) * b[:, :, 0] + b[:, :, 1]
+                primed = m2 & (idx[:, None] >= 2)
+                if nm in ("d2xdt2_max", "d2xdt2_extrema"):
+                    b[:, :, 2] = np.where(primed & (d > b[:, :, 2]), d, b[:, :, 2])
+                if nm == "d2xdt2_min":
+                    b[:, :, 2] = np.where(primed & (d < b[:, :, 2]), d, b[:, :, 2])
+                if nm == "d2xdt2_extrema":
+                    b[:, :, 3] = np.where(primed & (d < b[:, :, 3]), d, b[:, :, 3])
+                b[:, :, 1] = np.where(m2, b[:, :, 0], b[:, :, 1])
+                b[:, :, 0] = np.where(m2, vals, b[:, :, 0])
             elif nm == "peaks":
                 prev, pprev, pc = b[:, :, 0].copy(), b[:, :, 1].copy(), b[:, :, 2].astype(np.int64)
                 hit = m2 & (idx[:, None] >= 2) & (pc < par) & (pprev != 0) & (prev > vals) & (pprev < prev)
@@ -728,6 +760,16 @@ def integrate(system: OracleSystem, algorithm: str, inits: np.ndarray, params: n
                 b[:, :, 0] = np.where(m2, b[:, :, 0] + ms, b[:, :, 0])
                 b[:, :, 1] = np.where(m2, rt(0), b[:, :, 1])
                 b[:, :, 2] = np.where(m2, rt(0), b[:, :, 2])
+            elif nm.startswith("dxdt_") or nm.startswith("d2xdt2_"):
+                first = nm.startswith("dxdt_")
+                k0 = 1 if first else 2
+                scale = rt(samp_every) if first else rt(samp_every) * rt(samp_every)
+                hi_first = nm.endswith("_max") or nm.endswith("_extrema")
+                outs[:, :, ooff] = b[:, :, k0] / scale
+                b[:, :, k0] = np.where(m2, rt(-1e30) if hi_first else rt(1e30), b[:, :, k0])
+                if nm.endswith("_extrema"):
+                    outs[:, :, ooff + 1] = b[:, :, k0 + 1] / scale
+                    b[:, :, k0 + 1] = np.where(m2, rt(1e30), b[:, :, k0 + 1])
             elif nm == "peaks":
                 for q in range(par):
                     outs[:, :, ooff + q] = b[:, :, 3 + q]

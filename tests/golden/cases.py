@@ -196,6 +196,18 @@ CASES.update({
     "vdp_rodas3p_f64": dict(system=VDP, algorithm="rodas3p", precision="float64",
                             inputs=("vdp", 4, 50, [1.0, 3.0, 10.0, 30.0]), duration=1.0,
                             kwargs=dict(rtol=1e-7, atol=1e-7, save_every=0.25, output_types=_ITS)),
+    "fhn_dp54_derivs_f64": dict(system=FHN, algorithm="dormand-prince-54", precision="float64",
+                                inputs=("fhn", 4, 52), duration=30.0,
+                                kwargs=dict(rtol=1e-8, atol=1e-8, save_every=1.0, summarise_every=10.0,
+                                            sample_summaries_every=0.25,
+                                            output_types=["state", "time", "dxdt_max", "dxdt_min",
+                                                          "d2xdt2_max"])),
+    "fhn_dp54_derivs_f32": dict(system=FHN, algorithm="dormand-prince-54", precision="float32",
+                                inputs=("fhn", 4, 53), duration=30.0,
+                                kwargs=dict(rtol=1e-6, atol=1e-6, save_every=1.0, summarise_every=10.0,
+                                            sample_summaries_every=0.25,
+                                            output_types=["state", "time", "mean", "dxdt_min", "d2xdt2_max",
+                                                          "d2xdt2_min"])),
     "vdp_rosenbrock23_f32": dict(system=VDP, algorithm="rosenbrock23", precision="float32",
                                  inputs=("vdp", 4, 51, [1.0, 3.0, 10.0, 30.0]), duration=1.0,
                                  kwargs=dict(rtol=1e-5, atol=1e-5, save_every=0.25, output_types=_ITS)),
