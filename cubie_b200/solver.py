@@ -56,7 +56,8 @@ LOOP_KEYS = {"save_every", "summarise_every", "sample_summaries_every"}
 # the register-resident dense LU forms
 DIRECT_MAX_WIDTH = 16
 EXECUTION_KEYS = {"mixed_precision", "kernel", "block_size", "min_blocks_per_sm", "max_steps", "device", "fast_math",
-                  "precision", "adjoint", "layout", "schedule"}
+                  "precision", "adjoint", "layout", "schedule", "mem_proportion", "host_spill_threshold",
+                  "spill_dir", "max_chunk_runs"}
 IGNORED_KEYS = {"memory_settings", "cache", "auto_memory", "lineinfo", "time_logging_level",
                 "profileCUDA", "cache_settings"}
 RENAMED = {"dt_save": "save_every", "dt_summarise": "summarise_every",
@@ -151,6 +152,19 @@ class Solver:
         if self.schedule not in ("auto", "longest_first", "index"):
             raise ValueError("schedule must be 'auto', 'longest_first' or 'index'")
         self.max_steps = int(execution.get("max_steps", 0))
+        # memory: share of device memory a solve may hold (None: 90 % of
+        # free), outputs above host_spill_threshold bytes go to memory-mapped
+        # files in spill_dir, max_chunk_runs caps the runs per launch
+        mp = execution.get("mem_proportion")
+        self.mem_proportion = None if mp is None else float(mp)
+        if self.mem_proportion is not None and not 0.0 < self.mem_proportion <= 1.0:
+            raise ValueError("mem_proportion must be in (0, 1]")
+        hst = execution.get("host_spill_threshold")
+        self.host_spill_threshold = None if hst is None else int(hst)
+        self.spill_dir = execution.get("spill_dir")
+        mcr = execution.get("max_chunk_runs")
+        self.max_chunk_runs = None if mcr is None else int(mcr)
+        self.chunks = 1
         self.device = int(execution.get("device", 0))
         self.fast_math = bool(execution.get("fast_math", True))
         self._resolve_step_control(step)
@@ -555,6 +569,21 @@ class Solver:
         dev = torch.device("cuda", self.device)
         tdtype = torch.float32 if self.precision == np.float32 else torch.float64
         n_runs = int(inits.shape[1])
+        # run-axis chunking when the batch does not fit the memory budget
+        from . import chunking
+        plan = chunking.plan_chunks(
+            n_runs, chunking.bytes_per_run(self, prep, int(durations is not None) + int(tol_scale is not None)),
+            chunking.device_budget(self.device, self.mem_proportion), self.max_chunk_runs)
+        if plan.n_chunks > 1:
+            if on_device:
+                raise ValueError("a chunked run cannot return device arrays (on_device=True); raise "
+                                 "mem_proportion or solve fewer runs at a time")
+            coeff = None
+            if interp is not None:
+                coeff = torch.as_tensor(interp.coefficients.astype(self.precision), device=dev).contiguous()
+            return chunking.run_chunked(self, prep, inits, params, coeff, plan, duration, settling_time, t0,
+                                        durations, tol_scale, nan_error_trajectories)
+        self.chunks = 1
         inits_t = inits if isinstance(inits, torch.Tensor) else torch.as_tensor(np.ascontiguousarray(inits), device=dev)
         params_t = params if isinstance(params, torch.Tensor) else torch.as_tensor(np.ascontiguousarray(params), device=dev)
         inits_t = inits_t.to(device=dev, dtype=tdtype, non_blocking=True).contiguous()
@@ -638,7 +667,8 @@ class Solver:
         return torch.argsort(dur_t, descending=True).to(torch.int64).contiguous()
 
     def make_args(self, prep, bufs, inits_t, params_t, coeff_t, n_runs, duration, settling_time, t0,
-                  dur_t=None, tol_t=None, max_steps=None, order_t=None) -> "_native.SolveArgs":
+                  dur_t=None, tol_t=None, max_steps=None, order_t=None,
+                  run_stride=None) -> "_native.SolveArgs":
         def ptr(t):
             return t.data_ptr() if t is not None else None
         a = _native.SolveArgs()
@@ -659,7 +689,7 @@ class Solver:
         a.abort_flag = None
         a.run_order = ptr(order_t)
         a.n_runs = n_runs
-        a.run_stride = n_runs
+        a.run_stride = n_runs if run_stride is None else int(run_stride)
         a.max_steps = int(self.max_steps if max_steps is None else max_steps)
         a.duration = float(duration)
         a.warmup = float(settling_time)
@@ -671,32 +701,37 @@ class Solver:
         return a
 
     def collect(self, prep, bufs, n_runs, duration, settling_time, t0, nan_error_trajectories=True,
-                on_device=False) -> SolveResult:
+                on_device=False, host_arrays=None) -> SolveResult:
+        """Build the :class:`SolveResult` from the device buffers of a
+        launch (``bufs``), or from outputs already on the host
+        (``host_arrays``, same keys; the chunked path)."""
         spec: KernelSpec = prep["spec"]
-        if on_device:
-            conv = lambda t: t  # noqa: E731
+        keys = ("state", "obs", "state_sum", "obs_sum", "counters", "status", "totals")
+        if host_arrays is not None:
+            out = {k: host_arrays.get(k) for k in keys}
+        elif on_device:
+            out = {k: bufs.get(k) for k in keys}
         else:
             # one batch of asynchronous copies into pinned host memory (the
             # host caching allocator reuses the blocks across calls), then a
             # single wait: pageable copies would be staged through a bounce
             # buffer one output at a time
             torch = _torch()
-            host = {}
-            for key in ("state", "obs", "state_sum", "obs_sum", "counters", "status", "totals"):
+            pinned = {}
+            for key in keys:
                 t = bufs.get(key)
                 if t is not None:
-                    h = torch.empty(tuple(t.shape), dtype=t.dtype, pin_memory=True)
-                    h.copy_(t, non_blocking=True)
-                    host[id(t)] = h
+                    pinned[key] = torch.empty(tuple(t.shape), dtype=t.dtype, pin_memory=True)
+                    pinned[key].copy_(t, non_blocking=True)
             torch.cuda.current_stream(bufs["status"].device).synchronize()
-            conv = lambda t: host[id(t)].numpy() if t is not None else None  # noqa: E731
+            out = {k: (pinned[k].numpy() if k in pinned else None) for k in keys}
         res = SolveResult(
-            state=conv(bufs["state"]), observables=conv(bufs["obs"]),
-            state_summaries=conv(bufs["state_sum"]), observable_summaries=conv(bufs["obs_sum"]),
-            iteration_counters=conv(bufs["counters"]), status_codes=conv(bufs["status"]),
+            state=out["state"], observables=out["obs"],
+            state_summaries=out["state_sum"], observable_summaries=out["obs_sum"],
+            iteration_counters=out["counters"], status_codes=out["status"],
             save_time=spec.save_time,
         )
-        tot = conv(bufs["totals"]) if not on_device else bufs["totals"].cpu().numpy()
+        tot = out["totals"].cpu().numpy() if (on_device and host_arrays is None) else out["totals"]
         res.totals = dict(steps=int(tot[0]), rejections=int(tot[1]), newton=int(tot[2]), krylov=int(tot[3]))
         res.kernel_ms = self.last_kernel_ms
         sysm = self.system

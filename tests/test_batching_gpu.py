@@ -83,3 +83,41 @@ def test_longest_first_claims_leave_results_unchanged(cuda_device, lin):
     assert out["auto"].status_codes.tolist() == out["index"].status_codes.tolist()
     np.testing.assert_array_equal(out["auto"].state, out["index"].state)
     assert out["auto"].totals == out["index"].totals
+
+
+@pytest.mark.parametrize("per_run_horizons", [False, True])
+def test_chunked_solve_equals_unchunked(cuda_device, tmp_path, per_run_horizons):
+    """A batch forced into five chunks (``max_chunk_runs``), and the same
+    with outputs spilled to memory-mapped files, returns exactly what the
+    single launch returns: saved states, summaries, counters, statuses and
+    the launch totals (regular saves and summaries; or per-run horizons,
+    which save the final state only)."""
+    from cubie_b200 import Solver, create_ODE_system
+    sysm = create_ODE_system(VDP, states={"x": 2.0, "y": 0.0}, parameters={"mu": 10.0}, precision=np.float32)
+    kw = dict(algorithm="ros3p", rtol=1e-6, atol=1e-6, linear_correction_type="direct", mixed_precision=True)
+    if per_run_horizons:
+        kw["output_types"] = ["state", "iteration_counters"]
+    else:
+        kw.update(save_every=1.0, summarise_every=2.0, sample_summaries_every=0.5,
+                  output_types=["state", "time", "iteration_counters", "mean", "max"])
+    rng = np.random.default_rng(11)
+    n = 5000
+    mu = 10.0 ** rng.uniform(0, 2, n)
+    x0 = rng.uniform(-2, 2, (2, n))
+    solve_kw = dict(duration=8.0, nan_error_trajectories=False)
+    if per_run_horizons:
+        solve_kw["durations"] = np.minimum(2.0 * mu, 8.0)
+    whole = Solver(sysm, **kw).solve(x0, mu[None, :], **solve_kw)
+    chunked_solver = Solver(sysm, max_chunk_runs=1000, **kw)
+    chunked = chunked_solver.solve(x0, mu[None, :], **solve_kw)
+    assert chunked_solver.chunks == 5
+    spill_solver = Solver(sysm, max_chunk_runs=1000, host_spill_threshold=1, spill_dir=str(tmp_path), **kw)
+    spilled = spill_solver.solve(x0, mu[None, :], **solve_kw)
+    assert isinstance(spilled.state, np.memmap)
+    for res in (chunked, spilled):
+        assert res.status_codes.tolist() == whole.status_codes.tolist()
+        np.testing.assert_array_equal(res.state, whole.state)
+        if whole.state_summaries is not None:
+            np.testing.assert_array_equal(res.state_summaries, whole.state_summaries)
+        np.testing.assert_array_equal(res.iteration_counters, whole.iteration_counters)
+        assert res.totals == whole.totals
