@@ -73,6 +73,9 @@ class AdjointArgs(ctypes.Structure):
         ("lane_words", ctypes.c_longlong),
         ("ckpt_every", ctypes.c_int),
         ("max_ckpts", ctypes.c_int),
+        ("tape", ctypes.c_void_p),
+        ("tape_flags", ctypes.c_void_p),
+        ("step_count", ctypes.c_void_p),
     ]
 
 
@@ -93,7 +96,7 @@ EXPORTED = (
     "cbx_version", "cbx_last_error", "cbx_nvrtc_version", "cbx_compile", "cbx_free",
     "cbx_module_load", "cbx_module_create", "cbx_module_destroy", "cbx_kernel_info",
     "cbx_occupancy", "cbx_solve", "cbx_device_info", "cbx_fp32_peak_probe", "cbx_flush_l2",
-    "cbx_solve_noalloc", "cbx_adjoint_info", "cbx_adjoint_launch", "cbx_solve_hetero",
+    "cbx_solve_noalloc", "cbx_adjoint_info", "cbx_adjoint_tape_bytes", "cbx_adjoint_launch", "cbx_solve_hetero",
 )
 
 _lib = None
@@ -152,6 +155,7 @@ def lib():
                                        ctypes.c_void_p]
         L.cbx_adjoint_info.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong),
                                        ctypes.POINTER(ctypes.c_longlong)]
+        L.cbx_adjoint_tape_bytes.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong)]
         L.cbx_adjoint_launch.argtypes = [ctypes.c_void_p, ctypes.POINTER(SolveArgs), ctypes.POINTER(AdjointArgs),
                                          ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
         _lib = L
@@ -259,6 +263,12 @@ class Module:
         v, r = ctypes.c_longlong(), ctypes.c_longlong()
         _check(lib().cbx_adjoint_info(self._handle, ctypes.byref(v), ctypes.byref(r)), "cbx_adjoint_info")
         return v.value, r.value
+
+    def adjoint_tape_bytes(self) -> int:
+        """Bytes of one step-size tape entry (0: the module keeps no tape)."""
+        v = ctypes.c_longlong()
+        _check(lib().cbx_adjoint_tape_bytes(self._handle, ctypes.byref(v)), "cbx_adjoint_tape_bytes")
+        return v.value
 
     def adjoint_launch(self, args: SolveArgs, adj: AdjointArgs, phase: int, block: int, grid: int = 0,
                        stream: int = 0) -> None:

@@ -6,18 +6,21 @@ tableaus for autonomous systems without drivers) gets two extra kernels (``csrc/
 
 * the forward launch integrates every run exactly as the persistent kernel
   does, writes the same outputs, and stores the complete per-run loop state
-  every ``ckpt_every`` accepted steps;
+  every ``ckpt_every`` accepted steps (for explicit tableaus also a tape of
+  every accepted step's size and flags);
 * the backward launch replays each run segment by segment from those
-  checkpoints and back-propagates dL/d(saved state rows) through the
-  accepted steps (step sizes held fixed), giving dL/d(initial state) and
-  dL/d(parameters) for every run.
+  checkpoints (explicit tableaus: only the step function, driven by the
+  tape; Rosenbrock: the whole loop) and back-propagates dL/d(saved state
+  rows) through the accepted steps (step sizes held fixed), giving
+  dL/d(initial state) and dL/d(parameters) for every run.
 
 :class:`AdjointIntegrator` drives the two launches;
 :func:`solve_ivp_adjoint` wraps them in a ``torch.autograd.Function`` so a
 torch loss on the returned state tensor back-propagates into the initial
-values and parameters.  Memory: ``n_runs * max_ckpts`` checkpoint images
-plus one replay segment of ``ckpt_every`` records per run
-(:meth:`AdjointIntegrator.sizes` gives both sizes in bytes).  A run that
+values and parameters.  Memory: ``n_runs * max_ckpts`` checkpoint images,
+one replay segment of ``ckpt_every`` records per run and, for explicit
+tableaus, ``n_runs * max_ckpts * ckpt_every`` tape entries
+(:meth:`AdjointIntegrator.sizes` gives the three sizes in bytes).  A run that
 needs more than ``max_ckpts * ckpt_every`` accepted steps stops with
 status 32 (step budget), like ``max_steps``.
 """
@@ -47,8 +50,29 @@ class AdjointIntegrator:
         self.max_ckpts = int(max_ckpts)
 
     def sizes(self, prep) -> tuple:
-        """(bytes of one checkpoint image, bytes of one replay record)."""
-        return prep["module"].adjoint_sizes()
+        """(bytes of one checkpoint image, bytes of one replay record, bytes
+        of one tape entry or 0 when the configuration keeps no tape)."""
+        return prep["module"].adjoint_sizes() + (prep["module"].adjoint_tape_bytes(),)
+
+    def tape_layout(self, tape_entry: int) -> Tuple[int, int]:
+        """(entries, 32-bit flag words) of one run's step-size tape."""
+        cap = self.max_ckpts * self.ckpt_every
+        v = 16 // tape_entry
+        return -(-cap // v) * v, -(-cap // 32)
+
+    def _tape_buffers(self, n_runs: int, tape_entry: int, dev):
+        torch = _torch()
+        entries, words = self.tape_layout(tape_entry)
+        return (torch.empty((n_runs * entries * tape_entry // 4,), device=dev, dtype=torch.int32),
+                torch.empty((n_runs * words,), device=dev, dtype=torch.int32),
+                torch.empty((n_runs,), device=dev, dtype=torch.int32))
+
+    @staticmethod
+    def _set_tape(adj, tape) -> None:
+        if tape is None:
+            adj.tape = adj.tape_flags = adj.step_count = None
+        else:
+            adj.tape, adj.tape_flags, adj.step_count = (t.data_ptr() for t in tape)
 
     def forward(self, inits_t, params_t, duration: float, settling_time: float = 0.0, t0: float = 0.0,
                 stream=None):
@@ -67,20 +91,22 @@ class AdjointIntegrator:
             params_t = torch.zeros((1, max(n_runs, 1)), device=dev, dtype=tdtype)
         bufs = s.allocate_outputs(prep, n_runs, dev, tdtype)
         args = s.make_args(prep, bufs, inits_t, params_t, None, n_runs, duration, settling_time, t0)
-        lane, record = self.sizes(prep)
+        lane, record, tape_entry = self.sizes(prep)
         words = lane // 4
         ckpt = torch.empty((n_runs * self.max_ckpts * words,), device=dev, dtype=torch.int32)
         count = torch.zeros((n_runs,), device=dev, dtype=torch.int32)
+        tape = self._tape_buffers(n_runs, tape_entry, dev) if tape_entry > 0 else None
         adj = _native.AdjointArgs()
         adj.ckpt = ckpt.data_ptr()
         adj.ckpt_count = count.data_ptr()
         adj.lane_words = words
         adj.ckpt_every = self.ckpt_every
         adj.max_ckpts = self.max_ckpts
+        self._set_tape(adj, tape)
         st = stream if stream is not None else torch.cuda.current_stream(dev)
         prep["module"].adjoint_launch(args, adj, 0, s.block_size, 0, st.cuda_stream)
         saved = dict(prep=prep, bufs=bufs, inits=inits_t, params=params_t, ckpt=ckpt, count=count, words=words,
-                     record=record,
+                     record=record, tape=tape,
                      n_runs=n_runs, duration=duration, settling_time=settling_time, t0=t0, dev=dev, tdtype=tdtype)
         return bufs["state"], bufs["status"], saved
 
@@ -111,6 +137,7 @@ class AdjointIntegrator:
         adj.lane_words = saved["words"]
         adj.ckpt_every = self.ckpt_every
         adj.max_ckpts = self.max_ckpts
+        self._set_tape(adj, saved["tape"])
         st = stream if stream is not None else torch.cuda.current_stream(dev)
         prep["module"].adjoint_launch(args, adj, 1, s.block_size, 0, st.cuda_stream)
         return gi, (gp if npar > 0 else gp[:0])

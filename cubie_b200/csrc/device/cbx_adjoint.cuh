@@ -69,15 +69,22 @@ __device__ __forceinline__ void load_lane(Lane<Cfg>& L, const unsigned* src) {
 
 // One replayed step is one record of ``SegRecord<Cfg>::F`` values of the
 // system precision, contiguous per run, ``[run][step][F]``: the start state,
-// the start time, the step size and the saved output row (-1 if none; exact
-// as a floating value), padded to whole 16-byte vectors.  Lanes of a warp are
-// at different steps of different runs, so a record per lane moved with
-// 16-byte vector accesses costs one or two sectors per lane per step.
+// the start time (only when the right-hand side depends on time, directly or
+// through drivers) and the step size, negated when the step ends on a saved
+// output row, padded to whole 16-byte vectors.  Saved rows are consecutive,
+// so the reverse sweep recovers each row index by counting down from the
+// row count at the segment's end.  Lanes of a warp are at different steps
+// of different runs, so a record per lane moved with 16-byte vector
+// accesses costs one sector per lane per step for systems of up to three
+// states; the records of all resident lanes then stay within L2.
 template <class Cfg>
 struct SegRecord {
     using R = typename Cfg::R;
+    static constexpr bool TIMED = Cfg::ND > 0 || Cfg::Sys::HAS_DFDT;
+    static constexpr int T_AT = Cfg::N;                    // start time (TIMED only)
+    static constexpr int H_AT = Cfg::N + (TIMED ? 1 : 0);  // signed step size
     static constexpr int V = int(16 / sizeof(R));
-    static constexpr int F = ((Cfg::N + 3 + V - 1) / V) * V;
+    static constexpr int F = ((H_AT + 1 + V - 1) / V) * V;
     static __device__ __forceinline__ void store(R* dst, const R* rec) {
         if constexpr (sizeof(R) == 4) {
 #pragma unroll
@@ -114,21 +121,117 @@ struct SegRecord {
 template <class Cfg>
 struct SegRecorder {
     using R = typename Cfg::R;
+    using C = typename Cfg::C;
     static constexpr bool ACTIVE = true;
     static constexpr int F = SegRecord<Cfg>::F;
+    using Rec = SegRecord<Cfg>;
     R* seg;        // this run's records
     int count;
-    __device__ __forceinline__ void accepted(const Lane<Cfg>& L, R t, R h, int row) {
+    __device__ __forceinline__ void record(const R* y, R t, R h, bool saved) {
         R rec[F];
 #pragma unroll
-        for (int k = 0; k < Cfg::N; ++k) rec[k] = L.y[k];
-        rec[Cfg::N] = t;
-        rec[Cfg::N + 1] = h;
-        rec[Cfg::N + 2] = R(row);
+        for (int k = 0; k < Cfg::N; ++k) rec[k] = y[k];
+        if constexpr (Rec::TIMED) rec[Rec::T_AT] = t;
+        rec[Rec::H_AT] = saved ? -h : h;
 #pragma unroll
-        for (int k = Cfg::N + 3; k < F; ++k) rec[k] = R(0);
+        for (int k = Rec::H_AT + 1; k < F; ++k) rec[k] = R(0);
         SegRecord<Cfg>::store(seg + (long long)count * F, rec);
         ++count;
+    }
+    __device__ __forceinline__ void accepted(const Lane<Cfg>& L, C dt_eff, int row) {
+        record(L.y, R(L.tp), R(dt_eff), row >= 0);
+    }
+};
+
+// Step-size tape of the explicit Runge-Kutta adjoint.  For every accepted
+// step k of a run the checkpointing forward stores
+//   tape[run][k]        the step size as the loop advanced time with it
+//                       (control precision when the right-hand side depends
+//                       on time, else as the step function received it),
+//                       negated when the step ended on a saved output row;
+//   tape_flags[run][k / 32], bit k % 32: the attempt before it was rejected
+//                       (an FSAL tableau then re-evaluated its first stage
+//                       instead of reusing the last one);
+//   step_count[run]     the number of accepted steps.
+// Rows hold ``tape_row_entries(cap)`` entries and ``tape_flag_words(cap)``
+// words for cap = max_ckpts * ckpt_every.  Lanes of a warp are at different
+// steps of different runs, so the forward buffers entries in registers and
+// writes whole 16-byte vectors.  The reverse sweep replays a segment from its
+// checkpoint by calling the step function with those sizes, so the
+// controller, the event logic and the rejected attempts are not repeated.
+// An explicit step's result depends only on the start state, the step size,
+// the time and the two flags, so the replay is bit-identical to the forward.
+template <class Cfg>
+struct Tape {
+    using T = typename Pick<SegRecord<Cfg>::TIMED, typename Cfg::C, typename Cfg::R>::type;
+    static constexpr int V = int(16 / sizeof(T));   // entries per vector
+    static __host__ __device__ long long row_entries(long long cap) { return (cap + V - 1) / V * V; }
+    static __host__ __device__ long long flag_words(long long cap) { return (cap + 31) / 32; }
+    static __device__ __forceinline__ void store_vec(T* dst, const T* v) {
+        if constexpr (sizeof(T) == 4) {
+            *reinterpret_cast<float4*>(dst) = make_float4(v[0], v[1], v[2], v[3]);
+        } else {
+            *reinterpret_cast<double2*>(dst) = make_double2(v[0], v[1]);
+        }
+    }
+};
+
+// Explicit tableaus replay from the step-size tape; the others repeat the
+// loop (a Rosenbrock step's Krylov start depends on rejected attempts).
+template <class Cfg>
+struct UsesTape {
+    static constexpr bool VALUE = Cfg::ALGO == ALGO_ERK;
+};
+// Bytes of one tape entry, or 1 when the configuration keeps no tape (the
+// size of the module's ``cbx_tape_probe`` symbol).
+template <class Cfg>
+struct TapeBytes {
+    static constexpr int VALUE = UsesTape<Cfg>::VALUE ? int(sizeof(typename Tape<Cfg>::T)) : 1;
+};
+
+// Writes a run's tape from the forward loop's accepted steps.
+template <class Cfg>
+struct TapeRecorder {
+    using C = typename Cfg::C;
+    using T = typename Tape<Cfg>::T;
+    static constexpr int V = Tape<Cfg>::V;
+    static constexpr bool ACTIVE = true;
+    T* row;            // this run's entries
+    unsigned* flags;   // this run's rejected-attempt bits
+    T buf[V];          // entries of the current vector, newest last
+    unsigned rmask;    // bits of the current flag word
+    __device__ __forceinline__ void begin(T* r, unsigned* f) {
+        row = r;
+        flags = f;
+        rmask = 0u;
+#pragma unroll
+        for (int j = 0; j < V; ++j) buf[j] = T(0);
+    }
+    __device__ __forceinline__ void push(T v) {
+#pragma unroll
+        for (int j = 0; j < V - 1; ++j) buf[j] = buf[j + 1];
+        buf[V - 1] = v;
+    }
+    __device__ __forceinline__ void accepted(const Lane<Cfg>& L, C dt_eff, int saved_row) {
+        const int k = int(L.steps - L.rejections) - 1;   // below max_ckpts * ckpt_every
+        const T v = T(dt_eff);
+        push(saved_row >= 0 ? -v : v);
+        if (!L.prev_accepted) rmask |= 1u << (k & 31);
+        if ((k & (V - 1)) == V - 1) Tape<Cfg>::store_vec(row + (k - (V - 1)), buf);
+        if ((k & 31) == 31) {
+            flags[k >> 5] = rmask;
+            rmask = 0u;
+        }
+    }
+    // After the run's last accepted step (n in total): the partial vector
+    // and flag word.
+    __device__ __forceinline__ void finish(long long n) {
+        const int r = int(n % V);
+        if (r != 0) {
+            for (int j = r; j < V; ++j) push(T(0));
+            Tape<Cfg>::store_vec(row + (n - r), buf);
+        }
+        if ((n & 31) != 0) flags[n >> 5] = rmask;
     }
 };
 
@@ -143,12 +246,31 @@ struct ErkAdjoint {
     using Tab = typename Cfg::Tab;
     static constexpr int N = Cfg::N, S = Cfg::S, NP = Cfg::NP, ND = Cfg::ND;
 
-    // Stage i influences y+ when b_i != 0 or a later stage reads it.
-    static __host__ __device__ constexpr bool stage_used(int i) {
-        bool used = Tab::b(i) != 0.0;
-        for (int j = i + 1; j < S; ++j) used = used || (Tab::a(j, i) != 0.0);
-        return used;
+    // Stage i influences y+ when b_i != 0 or a later stage that influences
+    // y+ reads it (bit i of USED, filled from the last stage down).
+    static __host__ __device__ constexpr unsigned used_mask() {
+        unsigned m = 0u;
+        for (int i = S - 1; i >= 0; --i) {
+            bool used = Tab::b(i) != 0.0;
+            for (int j = i + 1; j < S; ++j) used = used || (Tab::a(j, i) != 0.0 && ((m >> j) & 1u));
+            if (used) m |= 1u << i;
+        }
+        return m;
     }
+    static constexpr unsigned USED = used_mask();
+    static __host__ __device__ constexpr bool stage_used(int i) { return (USED >> i) & 1u; }
+    // k_i must be recomputed when a later stage that itself matters reads it
+    // (Dormand-Prince's last stage only feeds the error estimate, so the
+    // stage before it needs no derivative here).
+    static __host__ __device__ constexpr unsigned feeds_mask() {
+        unsigned m = 0u;
+        for (int i = 0; i < S; ++i)
+            for (int j = i + 1; j < S; ++j)
+                if (Tab::a(j, i) != 0.0 && ((USED >> j) & 1u)) m |= 1u << i;
+        return m;
+    }
+    static constexpr unsigned FEEDS = feeds_mask();
+    static __host__ __device__ constexpr bool stage_feeds_used(int i) { return (FEEDS >> i) & 1u; }
 
     static __device__ __forceinline__ void reverse(const StepCtx<Cfg>& ctx, const R* y, R t, R h, R* lam,
                                                    C* pbar) {
@@ -167,15 +289,18 @@ struct ErkAdjoint {
                     if (j < i && Tab::a(i, j) != 0.0) acc += R(Tab::a(i, j)) * k[j][q];
                 Y[i][q] = (i == 0) ? y[q] : acc * h + y[q];
             }
-            if constexpr (ND > 0) Drivers<Cfg>::eval(stage_time, ctx.coeffs, drv_stage);
-            bool feeds_later = false;
-#pragma unroll
-            for (int j = 0; j < S; ++j)
-                if (j > i && Tab::a(j, i) != 0.0) feeds_later = true;
-            if (feeds_later) Sys::template dxdt<R>(Y[i], ctx.p, drv_stage, stage_time, k[i]);
+            if (stage_feeds_used(i)) {
+                if constexpr (ND > 0) Drivers<Cfg>::eval(stage_time, ctx.coeffs, drv_stage);
+                Sys::template dxdt<R>(Y[i], ctx.p, drv_stage, stage_time, k[i]);
+            }
         }
         R Ybar[S][N];
         R lam_out[N];
+        // this step's parameter sensitivity, summed over the stages in the
+        // working precision and added to the control-precision total once
+        R pstep[NP > 0 ? NP : 1];
+#pragma unroll
+        for (int q = 0; q < (NP > 0 ? NP : 1); ++q) pstep[q] = R(0);
 #pragma unroll
         for (int q = 0; q < N; ++q) lam_out[q] = lam[q];
 #pragma unroll
@@ -203,11 +328,15 @@ struct ErkAdjoint {
                 Sys::template pjac<R>(Y[i], ctx.p, drv_stage, stage_time, P);
                 Sys::template ptmv<R>(P, kbar, pb);
 #pragma unroll
-                for (int q = 0; q < NP; ++q) pbar[q] += C(pb[q]);
+                for (int q = 0; q < NP; ++q) pstep[q] += pb[q];
             }
         }
 #pragma unroll
         for (int q = 0; q < N; ++q) lam[q] = lam_out[q];
+        if constexpr (NP > 0) {
+#pragma unroll
+            for (int q = 0; q < NP; ++q) pbar[q] += C(pstep[q]);
+        }
     }
 };
 
@@ -369,11 +498,13 @@ struct StepAdjoint<Cfg, ALGO_ERK> : ErkAdjoint<Cfg> {};
 template <class Cfg>
 struct StepAdjoint<Cfg, ALGO_ROSENBROCK> : RosenbrockAdjoint<Cfg> {};
 
+
 // Forward integration with checkpoints (persistent work stealing, as
 // run_persistent).  A run that needs more than ``max_ckpts`` checkpoints
 // stops with status bit 32, like an exhausted step budget.
 template <class Cfg>
 __device__ __forceinline__ void run_adjoint_forward(const cbx_solve_args a, const cbx_adjoint_args g) {
+    using T = typename Tape<Cfg>::T;
     __shared__ BlockTotals bt;
     totals_begin(&bt);
     Lane<Cfg> L;
@@ -381,6 +512,8 @@ __device__ __forceinline__ void run_adjoint_forward(const cbx_solve_args a, cons
     int nck = 0;
     long long next_ck = 0;
     constexpr int W = LaneImage<Cfg>::WORDS;
+    const long long tape_cap = (long long)g.max_ckpts * g.ckpt_every;
+    TapeRecorder<Cfg> tr;
     while (true) {
         if (!active && !exhausted) {
             const long long run = claim_run(a.work_counter);
@@ -389,6 +522,9 @@ __device__ __forceinline__ void run_adjoint_forward(const cbx_solve_args a, cons
                 active = true;
                 nck = 0;
                 next_ck = 0;
+                if constexpr (UsesTape<Cfg>::VALUE)
+                    tr.begin(static_cast<T*>(g.tape) + run * Tape<Cfg>::row_entries(tape_cap),
+                             g.tape_flags + run * Tape<Cfg>::flag_words(tape_cap));
             } else {
                 exhausted = true;
             }
@@ -406,8 +542,16 @@ __device__ __forceinline__ void run_adjoint_forward(const cbx_solve_args a, cons
                     done = true;
                 }
             }
-            if (!done) done = lane_iterate<Cfg>(L, a);
+            if (!done) {
+                if constexpr (UsesTape<Cfg>::VALUE) done = lane_iterate<Cfg, TapeRecorder<Cfg>>(L, a, &tr);
+                else done = lane_iterate<Cfg>(L, a);
+            }
             if (done) {
+                if constexpr (UsesTape<Cfg>::VALUE) {
+                    const long long n = L.steps - L.rejections;
+                    tr.finish(n);
+                    g.step_count[L.run] = int(n);
+                }
                 lane_end<Cfg>(L, a, &bt);
                 g.ckpt_count[L.run] = nck;
                 active = false;
@@ -415,6 +559,35 @@ __device__ __forceinline__ void run_adjoint_forward(const cbx_solve_args a, cons
         }
     }
     totals_flush(&bt, a);
+}
+
+// One accepted step replayed from the tape: the step function with the
+// recorded size and flag, then the loop's own state commit and clock
+// update, recorded for the reverse pass.
+template <class Cfg>
+__device__ __forceinline__ void tape_step(Lane<Cfg>& L, typename Tape<Cfg>::T entry, bool prev_rejected,
+                                          SegRecorder<Cfg>& rec, const typename Cfg::R* coeffs) {
+    using R = typename Cfg::R;
+    using C = typename Cfg::C;
+    using T = typename Tape<Cfg>::T;
+    constexpr int N = Cfg::N, ND = Cfg::ND;
+    const bool saved = entry < T(0);
+    const T dt = saved ? -entry : entry;
+    const R h = R(dt);
+    rec.record(L.y, R(L.tp), h, saved);
+    L.save_idx += saved ? 1 : 0;   // rows are counted as the loop counts them
+    R ynew[N], delta[N], err[N];
+    R drv_new[ND > 0 ? ND : 1];
+    StepCtx<Cfg> ctx{L.p, coeffs, L.tol_scale};
+    Iters its;
+    Cfg::Step::step(ctx, L.y, ynew, delta, err, L.drv, drv_new, h, R(L.tp), L.first_step, !prev_rejected, L.ps,
+                    its);
+    L.first_step = false;
+    if constexpr (SegRecord<Cfg>::TIMED) {
+        L.t = L.t + double(dt);
+        L.tp = C(L.t);
+    }
+    commit_state<Cfg>(L, ynew, delta, drv_new);
 }
 
 template <class Cfg>
@@ -437,25 +610,29 @@ __device__ __forceinline__ void add_row_grad(typename Cfg::R* lam, const cbx_sol
 // previous checkpoint or, when its run is done, writes the gradients and
 // claims the next run.  Phases are warp-uniform, so the replay and the
 // reverse code never diverge against each other; lanes wait only for the
-// longest segment of the warp.
+// longest segment of the warp.  The loop state lives only inside one pass
+// (loaded from the checkpoint, replayed, dead once the records exist), so
+// the replay and the reverse step do not hold registers for each other.
 template <class Cfg>
 __device__ __forceinline__ void run_adjoint_backward(const cbx_solve_args a, const cbx_adjoint_args g) {
     using R = typename Cfg::R;
     using C = typename Cfg::C;
     using Adj = StepAdjoint<Cfg, Cfg::ALGO>;
-    constexpr int N = Cfg::N, NP = Cfg::NP, F = SegRecord<Cfg>::F;
+    using Rec = SegRecord<Cfg>;
+    using T = typename Tape<Cfg>::T;
+    constexpr int N = Cfg::N, NP = Cfg::NP, F = Rec::F;
     constexpr int W = LaneImage<Cfg>::WORDS;
     constexpr unsigned FULL = 0xffffffffu;
     const long long s = a.run_stride;
+    const long long tape_cap = (long long)g.max_ckpts * g.ckpt_every;
     cbx_solve_args replay = a;
     replay.n_save_rows = 0;      // the replay writes no outputs
     replay.n_summary_rows = 0;
     R* seg = static_cast<R*>(g.seg);
     const unsigned* ckpt = static_cast<const unsigned*>(g.ckpt);
-    Lane<Cfg> L;
-    SegRecorder<Cfg> rec{seg, 0};
+    constexpr int NPP = NP > 0 ? NP : 1;
     R lam[N];
-    C pbar[NP > 0 ? NP : 1];
+    C pbar[NPP];
     long long run = -1;
     int ck = -1;              // checkpoint of the segment in hand; -1: no run
     bool exhausted = false;
@@ -466,34 +643,85 @@ __device__ __forceinline__ void run_adjoint_backward(const cbx_solve_args a, con
 #pragma unroll
                 for (int q = 0; q < N; ++q) lam[q] = R(0);
 #pragma unroll
-                for (int q = 0; q < (NP > 0 ? NP : 1); ++q) pbar[q] = C(0);
+                for (int q = 0; q < NPP; ++q) pbar[q] = C(0);
                 ck = g.ckpt_count[run] - 1;
-                if (ck >= 0) load_lane<Cfg>(L, ckpt + (run * g.max_ckpts + ck) * (long long)W);
-                rec.seg = seg + run * (long long)g.ckpt_every * F;
-                rec.count = 0;
             } else {
                 exhausted = true;
             }
         }
         const bool busy = ck >= 0;
         if (!__any_sync(FULL, busy)) break;
-        // replay
-        bool replaying = busy;
-        while (__any_sync(FULL, replaying)) {
-            if (replaying) {
-                const bool done = lane_iterate<Cfg, SegRecorder<Cfg>>(L, replay, &rec);
-                if (done || rec.count >= g.ckpt_every) replaying = false;
+        R* const run_seg = seg + (busy ? run : 0) * (long long)g.ckpt_every * F;
+        R p[Cfg::NP > 0 ? Cfg::NP : 1];
+        C tol_scale;
+        int count, rows_end;
+        {
+            // replay
+            Lane<Cfg> L;
+            if (busy) load_lane<Cfg>(L, ckpt + (run * g.max_ckpts + ck) * (long long)W);
+            SegRecorder<Cfg> rec{run_seg, 0};
+            bool replaying = busy;
+            if constexpr (UsesTape<Cfg>::VALUE) {
+                // the segment's accepted steps from the tape, next entry in flight
+                const T* trow = static_cast<const T*>(g.tape) + (busy ? run : 0) * Tape<Cfg>::row_entries(tape_cap);
+                const unsigned* frow = g.tape_flags + (busy ? run : 0) * Tape<Cfg>::flag_words(tape_cap);
+                long long k = (long long)(busy ? ck : 0) * g.ckpt_every;
+                long long kend = 0;
+                if (busy) {
+                    const long long n = g.step_count[run];
+                    kend = k + g.ckpt_every < n ? k + g.ckpt_every : n;
+                }
+                T nxt = T(0);
+                unsigned word = 0u;
+                if (k < kend) {
+                    nxt = trow[k];
+                    word = frow[k >> 5];
+                }
+                while (__any_sync(FULL, replaying)) {
+                    if (replaying) {
+                        if (k >= kend) {
+                            replaying = false;
+                        } else {
+                            const T cur = nxt;
+                            const bool rej = ((word >> (k & 31)) & 1u) != 0u;
+                            if (k + 1 < kend) {
+                                nxt = trow[k + 1];
+                                if (((k + 1) & 31) == 0) word = frow[(k + 1) >> 5];
+                            }
+                            tape_step<Cfg>(L, cur, rej, rec, static_cast<const R*>(a.driver_coeffs));
+                            ++k;
+                        }
+                    }
+                }
+            } else {
+                while (__any_sync(FULL, replaying)) {
+                    if (replaying) {
+                        const bool done = lane_iterate<Cfg, SegRecorder<Cfg>>(L, replay, &rec);
+                        if (done || rec.count >= g.ckpt_every) replaying = false;
+                    }
+                }
             }
+#pragma unroll
+            for (int q = 0; q < (Cfg::NP > 0 ? Cfg::NP : 1); ++q) p[q] = busy ? L.p[q] : R(0);
+            tol_scale = busy ? L.tol_scale : C(1);
+            count = busy ? rec.count : 0;
+            rows_end = busy ? L.save_idx : 0;   // rows saved up to the segment's end
         }
-        // reverse
-        int j = busy ? rec.count - 1 : -1;
+        // reverse, with the next (earlier) record in flight
+        int j = count - 1;
+        R nxt[F];
+        if (j >= 0) Rec::load(run_seg + (long long)j * F, nxt);
         while (__any_sync(FULL, j >= 0)) {
             if (j >= 0) {
                 R rec_j[F];
-                SegRecord<Cfg>::load(rec.seg + (long long)j * F, rec_j);
-                add_row_grad<Cfg>(lam, a, g, int(rec_j[N + 2]), run);
-                StepCtx<Cfg> ctx{L.p, static_cast<const R*>(a.driver_coeffs), L.tol_scale};
-                Adj::reverse(ctx, rec_j, rec_j[N], rec_j[N + 1], lam, pbar);
+#pragma unroll
+                for (int k = 0; k < F; ++k) rec_j[k] = nxt[k];
+                if (j > 0) Rec::load(run_seg + (long long)(j - 1) * F, nxt);
+                const R hs = rec_j[Rec::H_AT];
+                if (hs < R(0)) add_row_grad<Cfg>(lam, a, g, --rows_end, run);
+                const R t = Rec::TIMED ? rec_j[Rec::T_AT] : R(0);
+                StepCtx<Cfg> ctx{p, static_cast<const R*>(a.driver_coeffs), tol_scale};
+                Adj::reverse(ctx, rec_j, t, fabs(hs), lam, pbar);
                 --j;
             }
         }
@@ -501,8 +729,6 @@ __device__ __forceinline__ void run_adjoint_backward(const cbx_solve_args a, con
         if (busy) {
             if (ck > 0) {
                 --ck;
-                load_lane<Cfg>(L, ckpt + (run * g.max_ckpts + ck) * (long long)W);
-                rec.count = 0;
             } else {
                 if (a.warmup == 0.0) add_row_grad<Cfg>(lam, a, g, 0, run);
                 R* gi = static_cast<R*>(g.grad_inits);
@@ -526,6 +752,7 @@ __device__ __forceinline__ void run_adjoint_backward(const cbx_solve_args a, con
 #define CBX_DEFINE_ADJOINT_KERNELS(CFG)                                                              \
     __constant__ char cbx_lane_probe[4 * cbx::LaneImage<CFG>::WORDS];                                         \
     __constant__ char cbx_seg_record_probe[sizeof(CFG::R) * cbx::SegRecord<CFG>::F];         \
+    __constant__ char cbx_tape_probe[cbx::TapeBytes<CFG>::VALUE];                                     \
     extern "C" __global__ void CBX_LAUNCH_BOUNDS(CFG) cbx_adjoint_forward(cbx_solve_args a,           \
                                                                          cbx_adjoint_args g) {       \
         cbx::run_adjoint_forward<CFG>(a, g);                                                          \

@@ -62,7 +62,16 @@ typedef struct cbx_solve_args {
  *   grad_state  [n_save_rows][n_saved_states + save_time][run_stride]:
  *               dL/d(saved state), same layout as state_out;
  *   grad_inits  [n_states][run_stride], grad_params [n_params][run_stride]:
- *               results (written, not accumulated).
+ *               results (written, not accumulated);
+ *   tape, tape_flags, step_count: explicit Runge-Kutta modules only
+ *               (cbx_adjoint_tape_bytes > 0), NULL otherwise; written by the
+ *               forward launch and read by the reverse sweep.  With
+ *               cap = max_ckpts * ckpt_every, e = cbx_adjoint_tape_bytes and
+ *               v = 16 / e: tape [run][ceil(cap / v) * v] entries of e bytes
+ *               (each accepted step's size, negated when it ended on a saved
+ *               row), tape_flags [run][ceil(cap / 32)] 32-bit words (bit set:
+ *               the attempt before that step was rejected), step_count [run]
+ *               int32 (accepted steps).
  */
 typedef struct cbx_adjoint_args {
     void* ckpt;
@@ -74,6 +83,9 @@ typedef struct cbx_adjoint_args {
     long long lane_words;       /* lane_bytes / 4 as reported by the module (a multiple of 4) */
     int ckpt_every;
     int max_ckpts;
+    void* tape;
+    unsigned* tape_flags;
+    int* step_count;
 } cbx_adjoint_args;
 
 /* Several configurations ("families") in one persistent launch.  Global

@@ -35,6 +35,19 @@ template <class T> __device__ __forceinline__ T clampv(T v, T lo, T hi) { return
 
 template <class T> __device__ __forceinline__ T absv(T v) { return v < T(0) ? -v : v; }
 
+// A round-to-nearest add the compiler never fuses with the multiply that
+// produced an operand.  Used where a value crosses from the step function
+// into the loop's state update: whether an FMA forms there otherwise depends
+// on the surrounding control flow, and the adjoint's replay must reproduce
+// the forward bit for bit from different surroundings.
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+
+// Type selection (A when B holds, else Bt) without the standard library,
+// which NVRTC does not provide.
+template <bool B, class A, class Bt> struct Pick { using type = A; };
+template <class A, class Bt> struct Pick<false, A, Bt> { using type = Bt; };
+
 __device__ __forceinline__ bool is_finite(float v) { return isfinite(v); }
 __device__ __forceinline__ bool is_finite(double v) { return isfinite(v); }
 __device__ __forceinline__ bool is_nan(float v) { return isnan(v); }

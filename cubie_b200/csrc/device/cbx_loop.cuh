@@ -184,6 +184,31 @@ __device__ __forceinline__ void lane_begin(Lane<Cfg>& L, const cbx_solve_args a,
     Step::init(L.ps);
 }
 
+// Accept a step's result: the state (compensated in the mixed-precision
+// mode: y + (delta + carried rounding)) and the drivers at its end.
+template <class Cfg>
+__device__ __forceinline__ void commit_state(Lane<Cfg>& L, const typename Cfg::R* ynew,
+                                             const typename Cfg::R* delta, const typename Cfg::R* drv_new) {
+    using R = typename Cfg::R;
+    constexpr int N = Cfg::N, ND = Cfg::ND;
+    if (Cfg::MIXED) {
+#pragma unroll
+        for (int i = 0; i < N; ++i) {
+            const R z = add_rn(delta[i], L.comp[i]);
+            const R ys = L.y[i] + z;
+            L.comp[i] = z - (ys - L.y[i]);
+            L.y[i] = ys;
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < N; ++i) L.y[i] = ynew[i];
+    }
+    if constexpr (ND > 0) {
+#pragma unroll
+        for (int q = 0; q < ND; ++q) L.drv[q] = drv_new[q];
+    }
+}
+
 // Observer of accepted steps (the adjoint's segment recorder); the default
 // observes nothing and compiles away.
 struct NoHook {
@@ -191,9 +216,12 @@ struct NoHook {
 };
 
 // One pass of the main loop body.  Returns true when the run is finished.
-// ``hook->accepted(L, t, h, row)`` sees every accepted step before the state
-// is updated: the step's start time and size exactly as the step function
-// received them, and the output row saved at its end (-1 if none).
+// ``hook->accepted(L, dt_eff, row)`` sees every accepted step before the
+// state is updated: ``L`` still holds the step's start (state, time, and the
+// first-step and previous-attempt flags the step function received),
+// ``dt_eff`` is the step size in the control precision (the step function
+// received it rounded to the system precision), ``row`` the output row saved
+// at its end (-1 if none).
 template <class Cfg, class Hook = NoHook>
 __device__ __forceinline__ bool lane_iterate(Lane<Cfg>& L, const cbx_solve_args a, Hook* hook = nullptr) {
     using R = typename Cfg::R;
@@ -297,26 +325,10 @@ __device__ __forceinline__ bool lane_iterate(Lane<Cfg>& L, const cbx_solve_args 
     if (L.irrecoverable) L.status |= L.iteration_status;
     if (accept) L.iteration_status = 0;
     if (accept) {
-        if constexpr (Hook::ACTIVE) hook->accepted(L, R(L.tp), R(dt_eff), do_save ? L.save_idx : -1);
+        if constexpr (Hook::ACTIVE) hook->accepted(L, dt_eff, do_save ? L.save_idx : -1);
         L.t = t_proposal;
         L.tp = C(L.t);
-        if (Cfg::MIXED) {
-            // compensated state update: y + (delta + carried rounding)
-#pragma unroll
-            for (int i = 0; i < N; ++i) {
-                const R z = delta[i] + L.comp[i];
-                const R ys = L.y[i] + z;
-                L.comp[i] = z - (ys - L.y[i]);
-                L.y[i] = ys;
-            }
-        } else {
-#pragma unroll
-            for (int i = 0; i < N; ++i) L.y[i] = ynew[i];
-        }
-        if constexpr (ND > 0) {
-#pragma unroll
-            for (int q = 0; q < ND; ++q) L.drv[q] = drv_new[q];
-        }
+        commit_state<Cfg>(L, ynew, delta, drv_new);
         if constexpr (NO > 0) Cfg::Sys::template observables<R>(L.y, L.p, L.drv, R(L.tp), L.obs);
     }
     L.prev_accepted = accept;

@@ -32,6 +32,7 @@ struct cbx_module {
     CUfunction adj[2];
     size_t lane_bytes;
     size_t record_bytes;
+    size_t tape_bytes;
     bool adj_resolved;
     int n_families;  // families of the heterogeneous kernel (0 without one)
 };
@@ -430,8 +431,13 @@ int resolve_adjoint(cbx_module* m) {
         int rc = check_cu(g_drv.cuModuleGetFunction(&m->adj[k], m->module, names[k]), names[k]);
         if (rc) return rc;
     }
+    // a module without the probe keeps no tape
+    CUdeviceptr probe3 = 0;
+    size_t tbytes = 0;
+    if (g_drv.cuModuleGetGlobal(&probe3, &tbytes, m->module, "cbx_tape_probe") != CUDA_SUCCESS) tbytes = 0;
     m->lane_bytes = bytes;
     m->record_bytes = rbytes;
+    m->tape_bytes = tbytes > 1 ? tbytes : 0;
     m->adj_resolved = true;
     return CBX_OK;
 }
@@ -444,6 +450,15 @@ extern "C" int cbx_adjoint_info(cbx_module* module, long long* lane_bytes, long 
     if (rc) return rc;
     *lane_bytes = (long long)module->lane_bytes;
     *record_bytes = (long long)module->record_bytes;
+    return CBX_OK;
+}
+
+extern "C" int cbx_adjoint_tape_bytes(cbx_module* module, long long* entry_bytes) {
+    if (!module || !entry_bytes) return fail(CBX_ERR_ARGUMENT, "null module or output pointer");
+    if (!load_driver()) return fail(CBX_ERR_NO_DEVICE, "CUDA driver library is not available");
+    int rc = resolve_adjoint(module);
+    if (rc) return rc;
+    *entry_bytes = (long long)module->tape_bytes;
     return CBX_OK;
 }
 
@@ -471,6 +486,9 @@ extern "C" int cbx_adjoint_launch(cbx_module* module, const cbx_solve_args* args
     }
     int rc = resolve_adjoint(module);
     if (rc) return rc;
+    if (module->tape_bytes > 0 && (!adj->tape || !adj->tape_flags || !adj->step_count))
+        return fail(CBX_ERR_ARGUMENT, "this module's adjoint needs a step-size tape, its flag words and step "
+                    "counts (%zu bytes per entry)", module->tape_bytes);
     if ((size_t)adj->lane_words * 4 < module->lane_bytes)
         return fail(CBX_ERR_ARGUMENT, "lane_words (%lld) is smaller than the module's lane image (%zu bytes)",
                     adj->lane_words, module->lane_bytes);

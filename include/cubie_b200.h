@@ -116,15 +116,22 @@ int cbx_flush_l2(void* buffer, size_t bytes, void* stream);
  * n_runs * ckpt_every * record_bytes, both 16-byte aligned, and pass
  * adj->lane_words = lane_bytes / 4.
  *
+ * cbx_adjoint_tape_bytes reports the size of one step-size tape entry:
+ * 4 or 8 for explicit Runge-Kutta modules, which then need adj->tape,
+ * adj->tape_flags and adj->step_count (sizes in cbx_args.h, 16-byte
+ * aligned), and 0 for the others (those three unused).
+ *
  * cbx_adjoint_launch with phase 0 integrates like cbx_solve's persistent
  * kernel (same outputs) and stores a checkpoint every adj->ckpt_every
- * accepted steps; a run needing more than adj->max_ckpts checkpoints stops
- * with status bit 32.  Phase 1, with the same args, the checkpoints of
- * phase 0, dL/d(saved state) in adj->grad_state and args->work_counter
- * zeroed again, writes dL/d(initial state) and dL/d(parameters) for every
- * run, holding the accepted step sizes fixed.  Both are asynchronous on
+ * accepted steps (and, with a tape, every accepted step's size); a run
+ * needing more than adj->max_ckpts checkpoints stops with status bit 32.
+ * Phase 1, with the same args, the checkpoints (and tape) of phase 0,
+ * dL/d(saved state) in adj->grad_state and args->work_counter zeroed
+ * again, writes dL/d(initial state) and dL/d(parameters) for every run,
+ * holding the accepted step sizes fixed.  Both are asynchronous on
  * ``stream``; grid = 0 picks a resident grid. */
 int cbx_adjoint_info(cbx_module* module, long long* lane_bytes, long long* record_bytes);
+int cbx_adjoint_tape_bytes(cbx_module* module, long long* entry_bytes);
 int cbx_adjoint_launch(cbx_module* module, const cbx_solve_args* args, const cbx_adjoint_args* adj,
                        int phase, int block, int grid, void* stream);
 

@@ -59,5 +59,9 @@ inline unsigned long long atomicAdd(unsigned long long* a, unsigned long long v)
 inline unsigned __activemask() { return 1u << (threadIdx.x & 31u); }
 inline int __ffs(unsigned v) { return v ? __builtin_ctz(v) + 1 : 0; }
 inline int __popc(unsigned v) { return __builtin_popcount(v); }
+// round-to-nearest adds that the device compiler never fuses into an FMA;
+// the host build contracts nothing, so they are plain adds here
+inline float __fadd_rn(float a, float b) { return a + b; }
+inline double __dadd_rn(double a, double b) { return a + b; }
 template <class T> inline T __shfl_sync(unsigned, T v, int) { return v; }
 inline bool __any_sync(unsigned, bool v) { return v; }

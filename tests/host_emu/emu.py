@@ -51,6 +51,7 @@ extern "C" void emu_adjoint(cbx_solve_args* a, cbx_adjoint_args* g, int phase, i
 }
 extern "C" long long emu_lane_bytes() { return (long long)sizeof(cbx_lane_probe); }
 extern "C" long long emu_record_bytes() { return (long long)sizeof(cbx_seg_record_probe); }
+extern "C" long long emu_tape_bytes() { return (long long)sizeof(cbx_tape_probe); }
 """
 
 HETERO_DRIVER = r"""
@@ -99,6 +100,7 @@ def compile_emulated(source: str):
         lib.emu_adjoint.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
         lib.emu_lane_bytes.restype = ctypes.c_longlong
         lib.emu_record_bytes.restype = ctypes.c_longlong
+        lib.emu_tape_bytes.restype = ctypes.c_longlong
     _cache[key] = lib
     return lib
 
@@ -193,6 +195,13 @@ def run_emulated_adjoint(solver, inits, params, duration, grad_state_fn, ckpt_ev
     ckpt = np.zeros((n_runs * max_ckpts * words,), np.uint32)
     count = np.zeros((n_runs,), np.int32)
     seg = np.zeros((ckpt_every * n_runs * int(lib.emu_record_bytes()) // 8 + 2,), np.float64)
+    tape_entry = int(lib.emu_tape_bytes())
+    tape_entry = tape_entry if tape_entry > 1 else 0
+    cap = max_ckpts * ckpt_every
+    v = 16 // tape_entry if tape_entry else 1
+    tape = np.zeros((max(n_runs * (-(-cap // v) * v) * tape_entry // 8, 2),), np.float64)
+    tape_flags = np.zeros((n_runs * (-(-cap // 32)),), np.uint32)
+    step_count = np.zeros((n_runs,), np.int32)
     gi = np.zeros((n, n_runs), p)
     gp = np.zeros((max(npar, 1), n_runs), p)
 
@@ -215,6 +224,8 @@ def run_emulated_adjoint(solver, inits, params, duration, grad_state_fn, ckpt_ev
     g.lane_words = words
     g.ckpt_every = ckpt_every
     g.max_ckpts = max_ckpts
+    if tape_entry > 0:
+        g.tape, g.tape_flags, g.step_count = tape.ctypes.data, tape_flags.ctypes.data, step_count.ctypes.data
     lib.emu_adjoint(ctypes.byref(a), ctypes.byref(g), 0, 1, 32)
     grad_state = np.ascontiguousarray(grad_state_fn(state), dtype=p)
     g.seg = seg.ctypes.data

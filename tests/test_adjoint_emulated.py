@@ -47,3 +47,43 @@ def test_rosenbrock_adjoint_emulated():
     ri, rp = _run(VDP, ["x", "y"], ["mu"], x0, p, 5.0, "ros3p", rtol=1e-9, atol=1e-9,
                   linear_correction_type="gmres", preconditioner_type=None)
     assert ri < 1e-5 and rp < 1e-5
+
+
+def test_erk_tape_replay_is_exact_with_time_dependence_and_rejections():
+    """The explicit adjoint replays segments from the step-size tape.  A
+    forced, time-dependent system at a loose tolerance (rejected attempts,
+    so first-stage re-evaluations) must give gradients that do not depend on
+    the checkpoint spacing at all (every spacing reconstructs the forward's
+    steps exactly), and that agree with the FP64 forward sensitivities to
+    the forward's own accuracy."""
+    from host_emu.emu import run_emulated_adjoint
+    from cubie_b200 import Solver, create_ODE_system
+    from oracle.sensitivity import SensitivitySystem, trajectory_gradients
+    eqs = ["dV = V - V**3 / 3 - w + I * (1 + 0.3 * sin(0.5 * t))", "dw = (V + a - b * w) / tau"]
+    states, params = ["V", "w"], ["a", "b", "tau", "I"]
+    rng = np.random.default_rng(5)
+    x0 = np.stack([rng.uniform(-1, 1, 3), rng.uniform(-0.5, 0.5, 3)])
+    p = np.stack([rng.uniform(0.5, 0.9, 3), rng.uniform(0.6, 1.0, 3), rng.uniform(8, 15, 3), rng.uniform(0.3, 0.6, 3)])
+    T = 30.0
+    target = rng.uniform(-1.0, 1.0, (int(T) + 1, 3))
+
+    def grad_fn(state):
+        g = np.zeros(state.shape)
+        g[:, 0, :] = 2.0 * (state[:, 0, :].astype(np.float64) - target) / target.size
+        return g
+
+    sysm = create_ODE_system(eqs, states={s: 0.0 for s in states}, parameters={q: 1.0 for q in params},
+                             precision=np.float64)
+    solver = Solver(sysm, algorithm="dormand-prince-54", output_types=["state"], save_every=1.0, adjoint=True,
+                    rtol=1e-5, atol=1e-5, dt=1.0)
+    results = [run_emulated_adjoint(solver, x0, p, T, grad_fn, ckpt_every=ce, max_ckpts=512)
+               for ce in (1, 5, 64)]
+    for state, status, gi, gp in results:
+        assert np.all(status == 0)
+        np.testing.assert_array_equal(gi, results[0][2])
+        np.testing.assert_array_equal(gp, results[0][3])
+    ssys = SensitivitySystem(eqs, states, params)
+    _, gy0, gpr = trajectory_gradients(ssys, x0, p, np.arange(int(T) + 1, dtype=float), grad_fn(results[0][0]))
+    gi, gp = results[0][2], results[0][3]
+    assert np.max(np.abs(gi - gy0)) / np.max(np.abs(gy0)) < 2e-3
+    assert np.max(np.abs(gp - gpr)) / np.max(np.abs(gpr)) < 2e-3

@@ -88,22 +88,27 @@ def test_rosenbrock_adjoint_matches_forward_sensitivities(cuda_device, lin):
     assert _rel(gp, gpr) < 1e-5
 
 
-def test_adjoint_is_independent_of_checkpoint_spacing(cuda_device):
+@pytest.mark.parametrize("mixed", [False, True])
+def test_adjoint_is_independent_of_checkpoint_spacing(cuda_device, mixed):
+    """Every spacing replays the forward's steps exactly (spacing 1 restarts
+    from a stored state at every step), so the gradients agree bit for bit;
+    the mixed-precision case covers the compensated state update."""
     import torch
     from cubie_b200.adjoint import AdjointIntegrator
     x0, p, rng = fhn_case(100, 5)
     solver = _solver(FHN, ["V", "w"], ["a", "b", "tau", "I"], np.float32, algorithm="dormand-prince-54",
-                     rtol=1e-6, atol=1e-6)
+                     rtol=1e-6, atol=1e-6, mixed_precision=mixed)
     xi = torch.tensor(x0, device="cuda", dtype=torch.float32)
     pi = torch.tensor(p, device="cuda", dtype=torch.float32)
     out = []
-    for every, cap in ((64, 64), (3, 4000)):
+    for every, cap in ((64, 64), (3, 4000), (1, 4000)):
         integ = AdjointIntegrator(solver, ckpt_every=every, max_ckpts=cap)
         state, status, saved = integ.forward(xi, pi, 20.0)
         g = torch.ones_like(state)
         out.append([t.cpu().numpy() for t in integ.backward(saved, g)] + [state.cpu().numpy(), status.cpu().numpy()])
-    for a, b in zip(out[0], out[1]):
-        np.testing.assert_array_equal(a, b)
+    for other in out[1:]:
+        for a, b in zip(out[0], other):
+            np.testing.assert_array_equal(a, b)
 
 
 def test_adjoint_forward_outputs_equal_solve(cuda_device):

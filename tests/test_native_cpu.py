@@ -32,8 +32,9 @@ def test_args_struct_layout_matches_header():
     from cubie_b200 import _native
     # 14 pointers, 3 int64, 5 float64, 2 int32
     assert ctypes.sizeof(_native.SolveArgs) == 15 * 8 + 3 * 8 + 5 * 8 + 2 * 4
-    # 6 pointers, 1 int64, 2 int32
-    assert ctypes.sizeof(_native.AdjointArgs) == 6 * 8 + 8 + 2 * 4
+    # 6 pointers, 1 int64, 2 int32, then the three tape pointers
+    assert ctypes.sizeof(_native.AdjointArgs) == 9 * 8 + 8 + 2 * 4
+    assert _native.AdjointArgs.tape.offset == 6 * 8 + 8 + 2 * 4
 
 
 def test_compile_error_is_reported():
