@@ -760,6 +760,8 @@ def main():
     ap.add_argument("--c3-steps", type=int, default=2)
     ap.add_argument("--adj-steps", type=int, default=3)
     ap.add_argument("--adj-warmup", type=int, default=3)
+    ap.add_argument("--leg", default=None, choices=["adjoint", "lorenz", "cable", "hetero"],
+                    help="run only this side leg on one GPU and print its record (for profiling)")
     args = ap.parse_args()
     for cfg in (NEW, NEW_RADAU):
         cfg["linear_correction_type"] = args.linear
@@ -768,6 +770,13 @@ def main():
     if args.impl == "reference":
         if rank == 0:
             print(json.dumps(reference_arm(args)), flush=True)
+        return
+    if args.leg is not None:
+        import torch
+        dev = torch.device("cuda", 0)
+        torch.cuda.set_device(dev)
+        arms = {"adjoint": adjoint_arm, "lorenz": lorenz_arm, "cable": cable_arm, "hetero": hetero_arm}
+        print(json.dumps({"leg": args.leg, **arms[args.leg](args, dev)}), flush=True)
         return
     dist = None
     if world > 1:

@@ -171,12 +171,19 @@ def run_emulated(solver, inits, params, duration, settling_time=0.0, t0=0.0, ker
     return bufs
 
 
-def run_emulated_adjoint(solver, inits, params, duration, grad_state_fn, ckpt_every=64, max_ckpts=64):
+def run_emulated_adjoint(solver, inits, params, duration, grad_state_fn, ckpt_every=64, max_ckpts=64,
+                         drivers=None):
     """Forward with checkpoints and the reverse sweep of the adjoint kernels
     on the CPU.  ``grad_state_fn(state)`` returns dL/d(state rows) for the
     forward's state output.  Returns (state, status, grad_inits, grad_params)."""
     from cubie_b200 import _native
-    prep = solver.prepare(duration, load=False)
+    interp = None
+    coeffs = None
+    if drivers is not None:
+        from cubie_b200.interpolator import ArrayInterpolator
+        interp = ArrayInterpolator.from_system(solver.system, drivers, solver.precision)
+        coeffs = np.ascontiguousarray(interp.coefficients, dtype=solver.precision)
+    prep = solver.prepare(duration, 0.0, 0.0, interp, None, load=False)
     spec = prep["spec"]
     lib = compile_emulated(prep["gen"].source)
     p = solver.precision
@@ -208,6 +215,7 @@ def run_emulated_adjoint(solver, inits, params, duration, grad_state_fn, ckpt_ev
     a = _native.SolveArgs()
     a.inits = inits.ctypes.data
     a.params = params.ctypes.data
+    a.driver_coeffs = coeffs.ctypes.data if coeffs is not None else None
     a.state_out = state.ctypes.data
     a.status_out = status.ctypes.data
     a.work_counter = work.ctypes.data
