@@ -5,6 +5,16 @@
 // cubie_b200/kernelgen.py).  Everything here is header-only device code.
 #pragma once
 
+// Functions whose body is large and called from many places (the class-
+// grouped right-hand side and J v of the warp layout) are kept as one copy:
+// inlined at every call site of every unrolled stage they multiplied the
+// kernel's code size until instruction fetch, not arithmetic, bounded it.
+#ifdef CBX_HOST_EMULATION
+#define CBX_NOINLINE __attribute__((noinline))
+#else
+#define CBX_NOINLINE __noinline__
+#endif
+
 namespace cbx {
 
 // Per-run status bits; values match the reference's CUBIE_RESULT_CODES

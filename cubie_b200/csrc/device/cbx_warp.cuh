@@ -208,7 +208,15 @@ struct WarpDirkStep {
         }
         ps.theta = C(0);
     }
-    static __device__ __forceinline__ int stage_solve(WarpCtx<Cfg>& w, R* base, const R* y, const R* drv_stage,
+    // Out of line: one copy of Newton + the Krylov solver serves every stage.
+    // Inlined into each unrolled stage, with the class-grouped f and J v
+    // bodies inlined at every call site, the 64-compartment cable's kernel
+    // held 246 KB of code and instruction fetch bounded it (the same time
+    // at 8 and at 12 resident warps per SM); as calls it holds 137 KB and
+    // runs 24 % faster.  Moving the operator and norm helpers out of line
+    // as well (98 KB) was slower again: their calls pass the per-lane
+    // vectors through the stack.
+    static __device__ CBX_NOINLINE int stage_solve(WarpCtx<Cfg>& w, R* base, const R* y, const R* drv_stage,
                                                       R stage_time, R dt, R a, Persist& ps, Iters& its) {
         WarpDirkProblem<Cfg> prob{&w, base, y, drv_stage, stage_time, dt, a};
         int ni = 0, ki = 0;

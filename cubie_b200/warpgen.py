@@ -116,7 +116,7 @@ def _emit_classes(name: str, classes: List[ExprClass], with_v: bool, tables: Lis
     """A device function evaluating every class for the calling lane."""
     lines = []
     fc = FlopCount()
-    sig = (f"    template <class R> static __device__ __forceinline__ void {name}(const R* __restrict__ ys, "
+    sig = (f"    template <class R> static __device__ CBX_NOINLINE void {name}(const R* __restrict__ ys, "
            + ("const R* __restrict__ vs, " if with_v else "")
            + "const R* __restrict__ ps, const R* __restrict__ ds, R t, R* __restrict__ out, int lane)")
     lines.append(sig)

@@ -19,7 +19,8 @@ def _build(nc, tmp_path):
     sysm = create_ODE_system(eqs, states=states, parameters=params, drivers=drivers, precision=np.float64)
     w = generate_warp_system(sysm)
     g = generate_system(sysm)
-    src = ("#include <cmath>\n#define __device__\n#define __forceinline__ inline\nusing std::exp; using std::pow;\n"
+    src = ("#include <cmath>\n#define __device__\n#define __forceinline__ inline\n"
+           "#define CBX_NOINLINE __attribute__((noinline))\nusing std::exp; using std::pow;\n"
            + g.source + "\n" + w.source + r'''
 extern "C" void eval(const double* y, const double* v, const double* p, const double* d, double t, double* f1,
                      double* f2, double* j1, double* j2) {
