@@ -601,14 +601,25 @@ def gpu_arm(args, rank: int, world: int, dist):
     x0_h = torch.as_tensor(x0.astype(np.float32)).pin_memory()
     mu_h = torch.as_tensor(mu[None, :].astype(np.float32)).pin_memory()
     du_h = torch.as_tensor(durs).pin_memory()
-    res = solver_e2e.solve(x0_h, mu_h, duration=float(durs.max()), durations=du_h, nan_error_trajectories=False)
-    e2e_times = []
-    for _ in range(max(1, args.steps)):
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
+    for _ in range(max(3, args.warmup)):
         res = solver_e2e.solve(x0_h, mu_h, duration=float(durs.max()), durations=du_h, nan_error_trajectories=False)
-        torch.cuda.synchronize()
-        e2e_times.append(time.perf_counter() - t0)
+    # wall-clock timing of the host API: Python's cyclic garbage collector is
+    # paused inside the timed calls (as timeit does), so a collection
+    # triggered by unrelated allocations does not land in one step
+    import gc
+    gc.collect()
+    gc.disable()
+    e2e_times = []
+    try:
+        for _ in range(max(1, args.steps)):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            res = solver_e2e.solve(x0_h, mu_h, duration=float(durs.max()), durations=du_h,
+                                   nan_error_trajectories=False)
+            torch.cuda.synchronize()
+            e2e_times.append(time.perf_counter() - t0)
+    finally:
+        gc.enable()
     log('e2e', e2e_times)
     e2e_frac, _ = solved_fraction(res.state[-1][:, :T], res.status_codes[:T])
     e2e_s, e2e_solved = aggregate(float(np.mean(e2e_times)), n * e2e_frac, device=dev)
