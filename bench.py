@@ -326,9 +326,10 @@ ROBERTSON = ["dy1 = -k1 * y1 + k3 * y2 * y3", "dy2 = k1 * y1 - k3 * y2 * y3 - k2
 
 def hetero_arm(args, dev):
     """2^20 runs split evenly by system: Lorenz (rho~U[20,35], x0~U[-10,10]^3;
-    DP54), stiff Van der Pol (mu=10^U[0,3], x0~U[-2,2]^2; ROS3P + GMRES) and
-    Robertson (k1=0.04, k2=3e7, k3=1e4 each x U[0.5,2], y0=(1,0,0); ROS3P +
-    GMRES); per-run rtol = 10^U[-8,-4] (a per-run scale on rtol 1e-4),
+    DP54), stiff Van der Pol (mu=10^U[0,3], x0~U[-2,2]^2; ROS3P) and
+    Robertson (k1=0.04, k2=3e7, k3=1e4 each x U[0.5,2], y0=(1,0,0); ROS3P),
+    the Rosenbrock stage systems solved by ``--linear`` (the in-register LU
+    by default); per-run rtol = 10^U[-8,-4] (a per-run scale on rtol 1e-4),
     per-run horizon 10^U[0,3]; FP32 stepping with FP64 time, control and
     norms; final state only; one heterogeneous persistent launch replayed as
     a CUDA graph.  Solved: status 0, and for Van der Pol and Robertson the
@@ -414,9 +415,9 @@ def hetero_arm(args, dev):
         solved_total += n * fam[name]["solved_fraction"]
     ms = float(np.mean(times))
     del flush
-    return {"workload": "2^20 runs split evenly: Lorenz DP54, stiff VdP ROS3P+GMRES, Robertson ROS3P+GMRES; per-run "
-                        "rtol 10^U[-8,-4], per-run horizon 10^U[0,3]; FP32 stepping + FP64 control; one "
-                        "heterogeneous persistent launch replayed as a CUDA graph",
+    return {"workload": f"2^20 runs split evenly: Lorenz DP54, stiff VdP ROS3P, Robertson ROS3P (stage systems: "
+                        f"{args.linear}); per-run rtol 10^U[-8,-4], per-run horizon 10^U[0,3]; FP32 stepping + FP64 "
+                        f"control; one heterogeneous persistent launch replayed as a CUDA graph",
             "n_systems": 3 * n, "ms": ms, "value": solved_total / (ms * 1e-3), "unit": "systems/s",
             "families": fam, "graph": True}
 
@@ -650,6 +651,19 @@ def gpu_arm(args, rank: int, world: int, dist):
         both = (plain["status"][:PT] == 0) & truth_ok[:PT] & (new["status"][:PT] == 0)
         matched = float(np.mean(err[:PT][both] <= np.maximum(p_err[both], 1.0))) if both.any() else None
 
+        # the configuration's literal linear solver: matrix-free GMRES
+        # (unpreconditioned) on the same persistent mixed-precision launch
+        gm = {}
+        for name, cfg in (("ros3p", NEW), ("radau", NEW_RADAU)):
+            if cfg["linear_correction_type"] == "gmres":
+                continue
+            g = device_timing(dict(cfg, linear_correction_type="gmres"), sys32, 1, 1, n)
+            g_ms = float(np.mean(g["times"]))
+            g_frac, _ = solved_fraction(g["y"][:, :T], g["status"][:T])
+            gm[name] = {"value": n * g_frac / (g_ms * 1e-3), "ms_per_step": g_ms, "solved_fraction": g_frac,
+                        "totals_per_step": g["totals"]}
+            log(f'{name}-gmres', g['times'], g['totals'])
+
         # the plain launch shape with the engine's algorithm settings
         same = device_timing(dict(NEW, kernel="plain"), sys32, 1, 1, n)
         s_ms = float(np.mean(same["times"]))
@@ -717,6 +731,8 @@ def gpu_arm(args, rank: int, world: int, dist):
                                 "matched_fraction = share of runs both kernels solved where the engine's "
                                 "error <= max(plain error, 1 tol unit)"},
             "speedup_vs_plain": value / plain_value if plain_value > 0 else None,
+            "gmres": dict(gm, config="linear_correction_type='gmres' (matrix-free, unpreconditioned), otherwise "
+                                      "the headline launch; 1 timed step after 1 warm-up"),
             "plain_same_settings": {"value": n * s_frac / (s_ms * 1e-3), "ms": s_ms, "solved_fraction": s_frac,
                                     "config": "plain one-thread-per-run launch, same algorithm and precision "
                                               "settings as the headline line"},
