@@ -9,10 +9,11 @@
 //             kernel does and additionally stores the complete per-run loop
 //             state (``Lane``) every ``ckpt_every`` accepted steps;
 //   reverse   ``cbx_adjoint_backward`` walks each run's checkpoints from
-//             last to first.  From checkpoint s it replays the loop (same
-//             code, same arithmetic, hence the same accepted steps) and
-//             records the start state, start time and size of the next
-//             ``ckpt_every`` accepted steps, then back-propagates
+//             last to first.  From checkpoint s it replays the next
+//             ``ckpt_every`` accepted steps bit for bit (explicit tableaus:
+//             the step function driven by the forward's step-size tape;
+//             Rosenbrock: the whole loop) and records each step's start
+//             state, start time and size, then back-propagates
 //             lambda = dL/dy through those steps in reverse order, adding
 //             dL/d(saved row) where a row was saved.  Parameter gradients
 //             accumulate in the control precision.
@@ -603,6 +604,29 @@ __device__ __forceinline__ void add_row_grad(typename Cfg::R* lam, const cbx_sol
     }
 }
 
+// dL/d(saved state) of one output row (zeros outside the saved rows), loaded
+// ahead of the reverse step that adds it.
+template <class Cfg>
+struct RowGrad {
+    using R = typename Cfg::R;
+    static constexpr int NS = Cfg::SAVE_STATE ? Cfg::N_SAVED_STATES : 0;
+    R v[NS > 0 ? NS : 1];
+    __device__ __forceinline__ void load(const cbx_solve_args& a, const cbx_adjoint_args& g, int row,
+                                         long long run) {
+        const bool in = row >= 0 && row < a.n_save_rows && g.grad_state;
+        if constexpr (NS > 0) {
+            constexpr int W = Cfg::N_SAVED_STATES + (Cfg::SAVE_TIME ? 1 : 0);
+            const R* gr = static_cast<const R*>(g.grad_state) + (long long)(in ? row : 0) * W * a.run_stride + run;
+#pragma unroll
+            for (int k = 0; k < NS; ++k) v[k] = in ? gr[k * a.run_stride] : R(0);
+        }
+    }
+    __device__ __forceinline__ void add_to(R* lam) const {
+#pragma unroll
+        for (int k = 0; k < NS; ++k) lam[Cfg::Idx::saved_state(k)] += v[k];
+    }
+};
+
 // Reverse sweep.  Every lane works on its own run, but a warp moves through
 // the phases together: all lanes replay their current segment (each until it
 // holds ``ckpt_every`` records or its run ends), then all lanes
@@ -707,10 +731,15 @@ __device__ __forceinline__ void run_adjoint_backward(const cbx_solve_args a, con
             count = busy ? rec.count : 0;
             rows_end = busy ? L.save_idx : 0;   // rows saved up to the segment's end
         }
-        // reverse, with the next (earlier) record in flight
+        // reverse, with the next (earlier) record and the next saved row's
+        // loss gradient (rows are met in decreasing order) in flight
         int j = count - 1;
         R nxt[F];
-        if (j >= 0) Rec::load(run_seg + (long long)j * F, nxt);
+        RowGrad<Cfg> row_next;
+        if (j >= 0) {
+            Rec::load(run_seg + (long long)j * F, nxt);
+            row_next.load(a, g, rows_end - 1, run);
+        }
         while (__any_sync(FULL, j >= 0)) {
             if (j >= 0) {
                 R rec_j[F];
@@ -718,7 +747,11 @@ __device__ __forceinline__ void run_adjoint_backward(const cbx_solve_args a, con
                 for (int k = 0; k < F; ++k) rec_j[k] = nxt[k];
                 if (j > 0) Rec::load(run_seg + (long long)(j - 1) * F, nxt);
                 const R hs = rec_j[Rec::H_AT];
-                if (hs < R(0)) add_row_grad<Cfg>(lam, a, g, --rows_end, run);
+                if (hs < R(0)) {
+                    row_next.add_to(lam);
+                    --rows_end;
+                    if (j > 0) row_next.load(a, g, rows_end - 1, run);
+                }
                 const R t = Rec::TIMED ? rec_j[Rec::T_AT] : R(0);
                 StepCtx<Cfg> ctx{p, static_cast<const R*>(a.driver_coeffs), tol_scale};
                 Adj::reverse(ctx, rec_j, t, fabs(hs), lam, pbar);
