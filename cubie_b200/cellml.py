@@ -1,0 +1,343 @@
+"""CellML models as :class:`~cubie_b200.symbolic.SymbolicODE` systems.
+
+Mirrors the reference's ``load_cellml_model``
+(``src/cubie/odesystems/symbolic/parsing/cellml.py:184``), which reads a
+model through a vendored copy of cellmlmanip (lxml, pint, rdflib).  Those
+libraries are not part of this engine; this loader reads the XML with the
+standard library and converts the MathML itself:
+
+* CellML 1.0, 1.1 and 2.0 documents (namespace picked from the root);
+* components, their variables and ``initial_value`` attributes (a number,
+  or in CellML 2.0 the name of a variable of the same component);
+* connections (``map_components`` / ``map_variables``): connected
+  variables are one model variable, named after the occurrence that
+  defines it (the one with an initial value or an equation);
+* MathML content markup: ``eq`` equations whose left side is a variable
+  (algebraic) or ``diff`` of a variable with respect to the time variable
+  (differential); ``plus minus times divide power root exp ln log abs
+  floor ceiling min max rem``, the trigonometric and hyperbolic functions
+  and their inverses, ``piecewise``/``piece``/``otherwise``, relations
+  (``eq neq lt gt leq geq``) and ``and or xor not``; ``cn`` in plain,
+  ``e-notation`` and ``integer`` forms; ``pi``, ``exponentiale``, ``true``,
+  ``false``, ``infinity``, ``notanumber``.
+
+Not done here: unit conversion (each variable is taken in the units its
+component declares, so connections between different but compatible
+units need the factor written into the model), ``reset`` and ``import``
+elements, and the reference's optional rewrite of removable
+Goldman-Hodgkin-Katz singularities (``U / (exp(U) - 1)`` is compiled as
+written; it is finite everywhere except exactly at ``U = 0``).
+
+States are the variables that have a ``diff`` equation; variables with an
+initial value and no equation are constants unless named in
+``parameters``; algebraic equations become auxiliaries, observables when
+named in ``observables``.  Names are the variables' own names, prefixed by
+their component (``component__name``) only where two model variables
+share a name.
+"""
+
+from __future__ import annotations
+
+import hashlib
+import re
+import xml.etree.ElementTree as ET
+from pathlib import Path
+from typing import Dict, List, Optional, Sequence, Tuple
+
+import numpy as np
+import sympy as sp
+
+from .symbolic import TIME, SymbolicODE, _topological
+
+MATHML = "http://www.w3.org/1998/Math/MathML"
+CELLML_NS = ("http://www.cellml.org/cellml/1.0#", "http://www.cellml.org/cellml/1.1#",
+             "http://www.cellml.org/cellml/2.0#")
+
+_UNARY = {
+    "exp": sp.exp, "ln": sp.log, "abs": sp.Abs, "floor": sp.floor, "ceiling": sp.ceiling,
+    "sin": sp.sin, "cos": sp.cos, "tan": sp.tan, "sec": sp.sec, "csc": sp.csc, "cot": sp.cot,
+    "sinh": sp.sinh, "cosh": sp.cosh, "tanh": sp.tanh, "sech": sp.sech, "csch": sp.csch, "coth": sp.coth,
+    "arcsin": sp.asin, "arccos": sp.acos, "arctan": sp.atan, "arcsec": sp.asec, "arccsc": sp.acsc,
+    "arccot": sp.acot, "arcsinh": sp.asinh, "arccosh": sp.acosh, "arctanh": sp.atanh,
+    "arcsech": sp.asech, "arccsch": sp.acsch, "arccoth": sp.acoth, "not": sp.Not,
+}
+_RELATIONS = {"eq": sp.Eq, "neq": sp.Ne, "lt": sp.Lt, "gt": sp.Gt, "leq": sp.Le, "geq": sp.Ge}
+_CONSTANTS = {"pi": sp.pi, "exponentiale": sp.E, "true": sp.true, "false": sp.false,
+              "infinity": sp.oo, "notanumber": sp.nan}
+
+
+def _local(tag: str) -> str:
+    return tag.rsplit("}", 1)[-1]
+
+
+def _sanitize(name: str) -> str:
+    s = re.sub(r"\W", "_", name)
+    return s if not s[0].isdigit() else "_" + s
+
+
+class _UnionFind:
+    def __init__(self):
+        self.parent: Dict[Tuple[str, str], Tuple[str, str]] = {}
+
+    def find(self, x):
+        self.parent.setdefault(x, x)
+        while self.parent[x] != x:
+            self.parent[x] = self.parent[self.parent[x]]
+            x = self.parent[x]
+        return x
+
+    def union(self, a, b):
+        ra, rb = self.find(a), self.find(b)
+        if ra != rb:
+            self.parent[rb] = ra
+
+
+class _MathML:
+    """MathML content markup of one component into SymPy."""
+
+    def __init__(self, resolve):
+        self.resolve = resolve  # local variable name -> SymPy symbol
+
+    def convert(self, el) -> sp.Expr:
+        tag = _local(el.tag)
+        if tag == "ci":
+            return self.resolve((el.text or "").strip())
+        if tag == "cn":
+            return self._number(el)
+        if tag in _CONSTANTS:
+            return _CONSTANTS[tag]
+        if tag == "apply":
+            return self._apply(list(el))
+        if tag == "piecewise":
+            pieces = []
+            otherwise = None
+            for child in el:
+                kind = _local(child.tag)
+                if kind == "piece":
+                    value, cond = list(child)
+                    pieces.append((self.convert(value), self.convert(cond)))
+                elif kind == "otherwise":
+                    otherwise = self.convert(list(child)[0])
+            pieces.append((otherwise if otherwise is not None else sp.nan, sp.true))
+            return sp.Piecewise(*pieces)
+        raise ValueError(f"unsupported MathML element <{tag}>")
+
+    @staticmethod
+    def _number(el) -> sp.Expr:
+        kind = el.get("type", "real")
+        parts = [el.text or ""] + [(c.tail or "") for c in el]
+        if kind == "e-notation":
+            mant, expo = (p.strip() for p in parts[:2])
+            return sp.Float(f"{mant}e{expo}", 17)
+        text = "".join(parts).strip()
+        if kind == "integer":
+            return sp.Integer(int(text))
+        if kind == "rational":
+            num, den = (p.strip() for p in parts[:2])
+            return sp.Rational(int(num), int(den))
+        value = float(text)
+        return sp.Integer(int(value)) if value.is_integer() and abs(value) < 2 ** 53 else sp.Float(text, 17)
+
+    def _apply(self, children) -> sp.Expr:
+        op = _local(children[0].tag)
+        qualifiers = {_local(c.tag): c for c in children[1:] if _local(c.tag) in ("degree", "logbase", "bvar")}
+        args = [self.convert(c) for c in children[1:] if _local(c.tag) not in ("degree", "logbase", "bvar")]
+        if op == "plus":
+            return sp.Add(*args)
+        if op == "minus":
+            return -args[0] if len(args) == 1 else args[0] - args[1]
+        if op == "times":
+            return sp.Mul(*args)
+        if op == "divide":
+            return args[0] / args[1]
+        if op == "power":
+            return args[0] ** args[1]
+        if op == "root":
+            degree = self.convert(list(qualifiers["degree"])[0]) if "degree" in qualifiers else sp.Integer(2)
+            return sp.sqrt(args[0]) if degree == 2 else args[0] ** (1 / degree)
+        if op == "log":
+            base = self.convert(list(qualifiers["logbase"])[0]) if "logbase" in qualifiers else sp.Integer(10)
+            return sp.log(args[0]) / sp.log(base)
+        if op == "rem":
+            return sp.Mod(args[0], args[1])
+        if op == "min":
+            return sp.Min(*args)
+        if op == "max":
+            return sp.Max(*args)
+        if op in _RELATIONS:
+            rel = [_RELATIONS[op](a, b) for a, b in zip(args[:-1], args[1:])]
+            return rel[0] if len(rel) == 1 else sp.And(*rel)
+        if op == "and":
+            return sp.And(*args)
+        if op == "or":
+            return sp.Or(*args)
+        if op == "xor":
+            return sp.Xor(*args)
+        if op in _UNARY:
+            return _UNARY[op](args[0])
+        raise ValueError(f"unsupported MathML operator <{op}>")
+
+
+def load_cellml_model(path, precision=np.float32, name: Optional[str] = None,
+                      parameters: Optional[Sequence[str]] = None, observables: Optional[Sequence[str]] = None,
+                      fix_singularities: bool = True, voltage_variable: Optional[str] = None,
+                      show_gui: bool = False) -> SymbolicODE:
+    """Read a CellML file into a :class:`SymbolicODE` (arguments as the
+    reference's ``load_cellml_model``).  ``parameters`` and ``observables``
+    name model variables (by their model name, or ``component__name``).
+    ``fix_singularities`` and ``voltage_variable`` are accepted for the same
+    call signature; no rewrite is applied (see the module notes).  The
+    constants editor GUI (``show_gui``) is not part of this engine."""
+    if not isinstance(path, (str, Path)):
+        raise TypeError("path must be a string or a Path")
+    path = Path(path)
+    if not path.exists():
+        raise FileNotFoundError(str(path))
+    if path.suffix != ".cellml":
+        raise ValueError(f"expected a .cellml file, got '{path.name}'")
+    if show_gui:
+        raise NotImplementedError("the constants editor GUI is not part of cubie_b200")
+    root = ET.parse(path).getroot()
+    ns = root.tag[1:].split("}", 1)[0] if root.tag.startswith("{") else ""
+    if ns not in CELLML_NS:
+        raise ValueError(f"not a CellML 1.0/1.1/2.0 model (root namespace '{ns}')")
+    cml = "{" + ns + "}"
+    v2 = ns.endswith("2.0#")
+
+    # variables per component
+    comps: Dict[str, Dict[str, dict]] = {}
+    uf = _UnionFind()
+    for comp in root.iter(cml + "component"):
+        cname = comp.get("name")
+        vars_ = {}
+        for var in comp.findall(cml + "variable"):
+            vars_[var.get("name")] = {"initial": var.get("initial_value")}
+            uf.find((cname, var.get("name")))
+        comps[cname] = vars_
+    for conn in root.iter(cml + "connection"):
+        if v2:
+            c1, c2 = conn.get("component_1"), conn.get("component_2")
+        else:
+            mc = conn.find(cml + "map_components")
+            c1, c2 = mc.get("component_1"), mc.get("component_2")
+        for mv in conn.findall(cml + "map_variables"):
+            uf.union((c1, mv.get("variable_1")), (c2, mv.get("variable_2")))
+
+    # equations per component, before naming (definitions decide names)
+    equations = []  # (component, kind, target local name, rhs element, time local name)
+    for cname in comps:
+        comp = next(c for c in root.iter(cml + "component") if c.get("name") == cname)
+        for math in comp.findall("{%s}math" % MATHML):
+            for ap in math:
+                kids = list(ap)
+                if _local(ap.tag) != "apply" or _local(kids[0].tag) != "eq":
+                    raise ValueError(f"component '{cname}': only <apply><eq/> equations are supported")
+                lhs, rhs = kids[1], kids[2]
+                if _local(lhs.tag) == "ci":
+                    equations.append((cname, "alg", lhs.text.strip(), rhs, None))
+                elif _local(lhs.tag) == "apply" and _local(list(lhs)[0].tag) == "diff":
+                    dk = list(lhs)
+                    bvar = next(c for c in dk if _local(c.tag) == "bvar")
+                    tname = list(bvar)[0].text.strip()
+                    target = next(c for c in dk[1:] if _local(c.tag) == "ci").text.strip()
+                    equations.append((cname, "ode", target, rhs, tname))
+                else:
+                    raise ValueError(f"component '{cname}': unsupported equation left-hand side")
+
+    # one model variable per connected class; its defining occurrence names it
+    classes: Dict[Tuple[str, str], List[Tuple[str, str]]] = {}
+    for cname, vars_ in comps.items():
+        for vname in vars_:
+            classes.setdefault(uf.find((cname, vname)), []).append((cname, vname))
+    defined = {uf.find((c, v)) for c, _, v, _, _ in equations}
+    time_classes = {uf.find((c, tname)) for c, kind, _, _, tname in equations if kind == "ode"}
+    if len(time_classes) > 1:
+        raise ValueError("differential equations use more than one time variable")
+
+    def source_of(members):
+        for c, v in members:
+            if comps[c][v]["initial"] is not None:
+                return c, v
+        for c, v in members:
+            if uf.find((c, v)) in defined:
+                for cc, _, vv, _, _ in equations:
+                    if (cc, vv) == (c, v):
+                        return c, v
+        return members[0]
+
+    sources = {root_: source_of(members) for root_, members in classes.items()}
+    counts: Dict[str, int] = {}
+    for root_, (c, v) in sources.items():
+        counts[v] = counts.get(v, 0) + 1
+    names = {root_: (_sanitize(v) if counts[v] == 1 else _sanitize(f"{c}__{v}")) for root_, (c, v) in sources.items()}
+    for root_ in time_classes:
+        names[root_] = "t"
+    reserved = {"t"}
+    for root_, nm in list(names.items()):
+        if root_ not in time_classes and nm in reserved | {"pi", "E", "e"}:
+            names[root_] = _sanitize(f"{sources[root_][0]}__{nm}")
+    symbols = {root_: (TIME if root_ in time_classes else sp.Symbol(nm, real=True)) for root_, nm in names.items()}
+
+    def initial(root_):
+        c, v = sources[root_]
+        val = comps[c][v]["initial"]
+        if val is None:
+            return None
+        try:
+            return float(val)
+        except ValueError:  # CellML 2.0: a variable of the same component
+            return initial(uf.find((c, val)))
+
+    derivatives: Dict[str, sp.Expr] = {}
+    assignments: List[Tuple[sp.Symbol, sp.Expr]] = []
+    states: Dict[str, float] = {}
+    algebraic = set()
+    for cname, kind, target, rhs, _ in equations:
+        conv = _MathML(lambda local, c=cname: symbols[uf.find((c, local))])
+        expr = conv.convert(rhs)
+        root_ = uf.find((cname, target))
+        if kind == "ode":
+            sname = names[root_]
+            if sname in derivatives:
+                raise ValueError(f"state '{sname}' has two differential equations")
+            derivatives[sname] = expr
+            states[sname] = initial(root_) if initial(root_) is not None else 0.0
+            assignments.append((sp.Symbol("d" + sname, real=True), expr))
+        else:
+            algebraic.add(root_)
+            assignments.append((symbols[root_], expr))
+    param_set = set(parameters or [])
+    obs_list = list(observables or [])
+    params: Dict[str, float] = {}
+    consts: Dict[str, float] = {}
+    state_roots = {uf.find((c, t)) for c, kind, t, _, _ in equations if kind == "ode"}
+    used = set()
+    for _, e in assignments:
+        used |= e.free_symbols
+    for root_, nm in names.items():
+        if root_ in time_classes or root_ in state_roots or root_ in algebraic:
+            continue
+        val = initial(root_)
+        if val is None and symbols[root_] not in used:
+            continue
+        if val is None:
+            raise ValueError(f"variable '{nm}' has neither a value nor an equation")
+        (params if nm in param_set else consts)[nm] = val
+    unknown = param_set - set(params)
+    if unknown:
+        raise ValueError(f"parameters {sorted(unknown)} are not constants of the model")
+    params = {nm: params[nm] for nm in (parameters or [])}   # the caller's order: the rows of a parameter array
+    alg_names = {names[r] for r in algebraic}
+    for o in obs_list:
+        if o not in alg_names:
+            raise ValueError(f"observable '{o}' is not defined by an algebraic equation")
+    base = set(states) | set(params) | set(consts) | {"t"}
+    assignments = _topological(assignments, base)
+    # derivative assignments go last, in state order, as the string front end builds them
+    aux = [(s, e) for s, e in assignments if not (s.name.startswith("d") and s.name[1:] in states)]
+    ders = [(sp.Symbol("d" + s, real=True), derivatives[s]) for s in states]
+    return SymbolicODE(states=states, parameters=params, constants=consts, drivers=[], observables=obs_list,
+                       assignments=aux + ders, derivatives=derivatives, precision=precision,
+                       name=name or path.stem,
+                       source="cellml:" + hashlib.sha256(path.read_bytes()).hexdigest() + "|P" + ",".join(params)
+                       + "|O" + ",".join(obs_list))

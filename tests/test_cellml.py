@@ -1,0 +1,218 @@
+"""CellML front end (cubie_b200.cellml.load_cellml_model).
+
+The models are written here, in CellML 1.0 and 2.0, for these tests.  The
+loaded systems are checked against the same equations given as strings
+(symbolically, and by integrating both with the emulated kernel), plus the
+loader's handling of connections, initial values given by name, piecewise
+definitions, e-notation numbers, parameters and observables."""
+
+import numpy as np
+import pytest
+import sympy as sp
+
+FHN = ["dV = V - V**3 / 3 - w + I", "dw = (V + a - b * w) / tau"]
+
+FHN_CELLML_10 = """<?xml version="1.0"?>
+<model xmlns="http://www.cellml.org/cellml/1.0#" xmlns:cellml="http://www.cellml.org/cellml/1.0#"
+       name="fhn_two_components">
+  <units name="ms"><unit units="second" prefix="milli"/></units>
+  <component name="environment">
+    <variable name="time" units="ms" public_interface="out"/>
+  </component>
+  <component name="membrane">
+    <variable name="time" units="ms" public_interface="in"/>
+    <variable name="V" units="dimensionless" initial_value="-1.2" public_interface="out"/>
+    <variable name="w_in" units="dimensionless" public_interface="in"/>
+    <variable name="I" units="dimensionless" initial_value="0.5"/>
+    <math xmlns="http://www.w3.org/1998/Math/MathML">
+      <apply><eq/>
+        <apply><diff/><bvar><ci>time</ci></bvar><ci>V</ci></apply>
+        <apply><plus/>
+          <apply><minus/><ci>V</ci>
+            <apply><divide/><apply><power/><ci>V</ci><cn cellml:units="dimensionless">3</cn></apply>
+              <cn cellml:units="dimensionless">3</cn></apply></apply>
+          <apply><minus/><ci>w_in</ci></apply>
+          <ci>I</ci>
+        </apply>
+      </apply>
+    </math>
+  </component>
+  <component name="recovery">
+    <variable name="time" units="ms" public_interface="in"/>
+    <variable name="V" units="dimensionless" public_interface="in"/>
+    <variable name="w" units="dimensionless" initial_value="0.6" public_interface="out"/>
+    <variable name="a" units="dimensionless" initial_value="0.7"/>
+    <variable name="b" units="dimensionless" initial_value="0.8"/>
+    <variable name="tau" units="ms" initial_value="1.25e1"/>
+    <math xmlns="http://www.w3.org/1998/Math/MathML">
+      <apply><eq/>
+        <apply><diff/><bvar><ci>time</ci></bvar><ci>w</ci></apply>
+        <apply><divide/>
+          <apply><minus/><apply><plus/><ci>V</ci><ci>a</ci></apply><apply><times/><ci>b</ci><ci>w</ci></apply></apply>
+          <ci>tau</ci></apply>
+      </apply>
+    </math>
+  </component>
+  <connection><map_components component_1="environment" component_2="membrane"/>
+    <map_variables variable_1="time" variable_2="time"/></connection>
+  <connection><map_components component_1="environment" component_2="recovery"/>
+    <map_variables variable_1="time" variable_2="time"/></connection>
+  <connection><map_components component_1="membrane" component_2="recovery"/>
+    <map_variables variable_1="V" variable_2="V"/>
+    <map_variables variable_1="w_in" variable_2="w"/></connection>
+</model>
+"""
+
+GATE_CELLML_20 = """<?xml version="1.0"?>
+<model xmlns="http://www.cellml.org/cellml/2.0#" xmlns:cellml="http://www.cellml.org/cellml/2.0#" name="gate">
+  <component name="main">
+    <variable name="t" units="ms" interface="public"/>
+    <variable name="x" units="dimensionless" initial_value="x0"/>
+    <variable name="x0" units="dimensionless" initial_value="0.25"/>
+    <variable name="V" units="mV" initial_value="-20"/>
+    <variable name="k" units="per_ms" initial_value="3"/>
+    <variable name="alpha" units="per_ms"/>
+    <variable name="drive" units="dimensionless"/>
+    <math xmlns="http://www.w3.org/1998/Math/MathML">
+      <apply><eq/><ci>alpha</ci>
+        <piecewise>
+          <piece><apply><times/><cn cellml:units="per_ms" type="e-notation">2.5<sep/>-1</cn>
+              <apply><exp/><apply><divide/><ci>V</ci><cn cellml:units="mV">10</cn></apply></apply></apply>
+            <apply><lt/><ci>V</ci><cn cellml:units="mV">0</cn></apply></piece>
+          <otherwise><apply><root/><degree><cn cellml:units="dimensionless">2</cn></degree><ci>k</ci></apply></otherwise>
+        </piecewise>
+      </apply>
+      <apply><eq/><ci>drive</ci><apply><sin/><apply><times/><pi/><ci>t</ci></apply></apply></apply>
+      <apply><eq/>
+        <apply><diff/><bvar><ci>t</ci></bvar><ci>x</ci></apply>
+        <apply><plus/>
+          <apply><times/><ci>alpha</ci><apply><minus/><cn cellml:units="dimensionless">1</cn><ci>x</ci></apply></apply>
+          <apply><times/><cn cellml:units="dimensionless">0.1</cn><ci>drive</ci></apply>
+          <apply><minus/><apply><times/><ci>k</ci><ci>x</ci></apply></apply>
+        </apply>
+      </apply>
+    </math>
+  </component>
+</model>
+"""
+
+
+def _write(tmp_path, text, name):
+    p = tmp_path / name
+    p.write_text(text)
+    return p
+
+
+def test_fhn_components_and_connections(tmp_path):
+    from cubie_b200 import create_ODE_system
+    from cubie_b200.cellml import load_cellml_model
+    ode = load_cellml_model(_write(tmp_path, FHN_CELLML_10, "fhn.cellml"), precision=np.float64,
+                            parameters=["a", "tau"])
+    assert ode.state_names == ["V", "w"]
+    assert ode.initial_values == {"V": -1.2, "w": 0.6}
+    assert ode.parameters == {"a": 0.7, "tau": 12.5}
+    assert ode.constants == {"I": 0.5, "b": 0.8}
+    ref = create_ODE_system(FHN, states={"V": -1.2, "w": 0.6}, parameters={"a": 0.7, "tau": 12.5},
+                            constants={"I": 0.5, "b": 0.8}, precision=np.float64)
+    names = {s.name: s for s in set().union(*[e.free_symbols for e in ref.derivatives.values()])}
+    for st in ("V", "w"):
+        mine = ode.derivatives[st].subs({s: names.get(s.name, s) for s in ode.derivatives[st].free_symbols})
+        assert sp.simplify(mine - ref.derivatives[st]) == 0
+
+
+def test_fhn_integrates_like_the_string_system(tmp_path):
+    from host_emu.emu import run_emulated
+    from cubie_b200 import Solver, create_ODE_system
+    from cubie_b200.cellml import load_cellml_model
+    ode = load_cellml_model(_write(tmp_path, FHN_CELLML_10, "fhn.cellml"), precision=np.float64,
+                            parameters=["a", "b", "tau", "I"])
+    ref = create_ODE_system(FHN, states={"V": -1.2, "w": 0.6}, parameters={"a": 0.7, "b": 0.8, "tau": 12.5, "I": 0.5},
+                            precision=np.float64)
+    rng = np.random.default_rng(3)
+    x0 = np.stack([rng.uniform(-1, 1, 4), rng.uniform(-0.5, 0.5, 4)])
+    p = np.stack([rng.uniform(0.5, 0.9, 4), rng.uniform(0.6, 1.0, 4), rng.uniform(8, 15, 4), rng.uniform(0.3, 0.6, 4)])
+    out = []
+    for sysm in (ode, ref):
+        s = Solver(sysm, algorithm="dormand-prince-54", rtol=1e-9, atol=1e-9, save_every=1.0, output_types=["state"])
+        out.append(run_emulated(s, x0, p, 20.0)["state"])
+    np.testing.assert_allclose(out[0], out[1], rtol=1e-12, atol=1e-12)
+
+
+def test_cellml2_piecewise_initial_by_name_and_observables(tmp_path):
+    from cubie_b200.cellml import load_cellml_model
+    ode = load_cellml_model(_write(tmp_path, GATE_CELLML_20, "gate.cellml"), precision=np.float64,
+                            observables=["alpha"])
+    assert ode.state_names == ["x"] and ode.initial_values == {"x": 0.25}
+    assert ode.observable_names == ["alpha"]
+    assert set(ode.constants) == {"x0", "V", "k"}
+    d = ode.derivatives["x"]
+    t = [s for s in d.free_symbols if s.name == "t"] or [sp.Symbol("t", real=True)]
+    alpha = {s.name: e for s, e in ode.assignments}["alpha"]
+    sub = {s: v for s in alpha.free_symbols | d.free_symbols for n, v in (("V", -20.0), ("k", 3.0)) if s.name == n}
+    assert float(alpha.subs(sub)) == pytest.approx(0.25 * np.exp(-2.0))
+    sub_pos = {s: (15.0 if s.name == "V" else 3.0) for s in alpha.free_symbols}
+    assert float(alpha.subs(sub_pos)) == pytest.approx(np.sqrt(3.0))
+    # dx/dt at x = 0.25, t = 0.5 with V = -20
+    vals = {"x": 0.25, "t": 0.5, "V": -20.0, "k": 3.0}
+    expr = d
+    for s, e in ode.assignments:
+        if s.name in ("alpha", "drive"):
+            expr = expr.subs(s, e)
+    got = float(expr.subs({s: vals[s.name] for s in expr.free_symbols}))
+    want = 0.25 * np.exp(-2.0) * 0.75 + 0.1 * np.sin(np.pi * 0.5) - 3.0 * 0.25
+    assert got == pytest.approx(want, rel=1e-12)
+
+
+def test_loader_errors(tmp_path):
+    from cubie_b200.cellml import load_cellml_model
+    with pytest.raises(FileNotFoundError):
+        load_cellml_model(tmp_path / "missing.cellml")
+    with pytest.raises(ValueError, match=".cellml"):
+        load_cellml_model(_write(tmp_path, FHN_CELLML_10, "fhn.xml"))
+    with pytest.raises(ValueError, match="not constants"):
+        load_cellml_model(_write(tmp_path, FHN_CELLML_10, "fhn.cellml"), parameters=["V"])
+    with pytest.raises(ValueError, match="observable"):
+        load_cellml_model(_write(tmp_path, FHN_CELLML_10, "fhn.cellml"), observables=["a"])
+
+
+@pytest.mark.gpu
+def test_cellml_model_solves_on_the_gpu_like_the_string_system(tmp_path, cuda_device):
+    from cubie_b200 import Solver, create_ODE_system
+    from cubie_b200.cellml import load_cellml_model
+    ode = load_cellml_model(_write(tmp_path, FHN_CELLML_10, "fhn.cellml"), precision=np.float64,
+                            parameters=["a", "b", "tau", "I"])
+    ref = create_ODE_system(FHN, states={"V": -1.2, "w": 0.6}, parameters={"a": 0.7, "b": 0.8, "tau": 12.5, "I": 0.5},
+                            precision=np.float64)
+    rng = np.random.default_rng(4)
+    x0 = np.stack([rng.uniform(-1, 1, 256), rng.uniform(-0.5, 0.5, 256)])
+    p = np.stack([rng.uniform(0.5, 0.9, 256), rng.uniform(0.6, 1.0, 256), rng.uniform(8, 15, 256),
+                  rng.uniform(0.3, 0.6, 256)])
+    res = [Solver(sysm, algorithm="dormand-prince-54", rtol=1e-9, atol=1e-9, save_every=1.0,
+                  output_types=["state"]).solve(x0, p, duration=20.0) for sysm in (ode, ref)]
+    assert np.all(res[0].status_codes == 0)
+    np.testing.assert_allclose(res[0].state, res[1].state, rtol=1e-10, atol=1e-12)
+
+
+def test_cellml2_model_compiles_and_integrates(tmp_path):
+    """The piecewise / sin / root model through code generation: NVRTC
+    compiles it for sm_100a and the emulated kernel matches SciPy."""
+    from scipy.integrate import solve_ivp as scipy_ivp
+    from host_emu.emu import run_emulated
+    from cubie_b200 import Solver, _native
+    from cubie_b200.cellml import load_cellml_model
+    ode = load_cellml_model(_write(tmp_path, GATE_CELLML_20, "gate.cellml"), precision=np.float64,
+                            parameters=["V", "k"])
+    s = Solver(ode, algorithm="dormand-prince-54", rtol=1e-10, atol=1e-10, save_every=0.5, output_types=["state"])
+    gk = s._generate(s.kernel_spec(s._timing(2.0)))
+    _native.compile_cubin(gk.source, _native.default_options(), use_cache=False)
+    V = np.array([-20.0, 15.0])
+    k = np.array([3.0, 1.5])
+    got = run_emulated(s, np.full((1, 2), 0.25), np.stack([V, k]), 2.0)["state"][:, 0, :]
+
+    def rhs(t, x, v, kk):
+        alpha = 0.25 * np.exp(v / 10.0) if v < 0 else np.sqrt(kk)
+        return [alpha * (1 - x[0]) + 0.1 * np.sin(np.pi * t) - kk * x[0]]
+
+    for j in range(2):
+        ref = scipy_ivp(rhs, (0, 2.0), [0.25], args=(V[j], k[j]), t_eval=np.arange(5) * 0.5, rtol=1e-12, atol=1e-12)
+        np.testing.assert_allclose(got[:, j], ref.y[0], rtol=1e-8, atol=1e-9)
