@@ -58,7 +58,8 @@ typedef struct cbx_solve_args {
  *   ckpt_count  [run] int32: slots written by the forward launch;
  *   seg         [run][ckpt_every][record_bytes]: one record per accepted
  *               step of the segment being replayed (start state, start
- *               time, step size, saved row), system precision;
+ *               time when f depends on time, step size negated on steps
+ *               that end on a saved row), system precision;
  *   grad_state  [n_save_rows][n_saved_states + save_time][run_stride]:
  *               dL/d(saved state), same layout as state_out;
  *   grad_inits  [n_states][run_stride], grad_params [n_params][run_stride]:
