@@ -24,7 +24,8 @@ standard library and converts the MathML itself:
 Not done here: unit conversion (each variable is taken in the units its
 component declares, so connections between different but compatible
 units need the factor written into the model), ``reset`` and ``import``
-elements, and the reference's optional rewrite of removable
+elements (both rejected with ``NotImplementedError``), and the reference's
+optional rewrite of removable
 Goldman-Hodgkin-Katz singularities (``U / (exp(U) - 1)`` is compiled as
 written; it is finite everywhere except exactly at ``U = 0``).
 
@@ -203,6 +204,10 @@ def load_cellml_model(path, precision=np.float32, name: Optional[str] = None,
         raise ValueError(f"not a CellML 1.0/1.1/2.0 model (root namespace '{ns}')")
     cml = "{" + ns + "}"
     v2 = ns.endswith("2.0#")
+    if root.find(cml + "import") is not None:
+        raise NotImplementedError("CellML imports are not supported: flatten the model into one document first")
+    if any(True for _ in root.iter(cml + "reset")):
+        raise NotImplementedError("CellML reset rules are not supported")
 
     # variables per component
     comps: Dict[str, Dict[str, dict]] = {}

@@ -216,3 +216,18 @@ def test_cellml2_model_compiles_and_integrates(tmp_path):
     for j in range(2):
         ref = scipy_ivp(rhs, (0, 2.0), [0.25], args=(V[j], k[j]), t_eval=np.arange(5) * 0.5, rtol=1e-12, atol=1e-12)
         np.testing.assert_allclose(got[:, j], ref.y[0], rtol=1e-8, atol=1e-9)
+
+
+def test_cellml11_namespace_and_unsupported_elements(tmp_path):
+    from cubie_b200.cellml import load_cellml_model
+    v11 = FHN_CELLML_10.replace("cellml/1.0#", "cellml/1.1#")
+    ode = load_cellml_model(_write(tmp_path, v11, "fhn11.cellml"))
+    assert ode.state_names == ["V", "w"]
+    imported = v11.replace('<component name="environment">',
+                           '<import xmlns:xlink="http://www.w3.org/1999/xlink" xlink:href="other.cellml"/>'
+                           '<component name="environment">')
+    with pytest.raises(NotImplementedError, match="imports"):
+        load_cellml_model(_write(tmp_path, imported, "imp.cellml"))
+    reset = GATE_CELLML_20.replace("</component>", "<reset variable=\"x\" test_variable=\"x\" order=\"1\"/></component>")
+    with pytest.raises(NotImplementedError, match="reset"):
+        load_cellml_model(_write(tmp_path, reset, "reset.cellml"))
