@@ -89,13 +89,19 @@ class AdjointIntegrator:
         params_t = params_t.detach().to(device=dev, dtype=tdtype).contiguous()
         if params_t.numel() == 0:
             params_t = torch.zeros((1, max(n_runs, 1)), device=dev, dtype=tdtype)
-        bufs = s.allocate_outputs(prep, n_runs, dev, tdtype)
-        args = s.make_args(prep, bufs, inits_t, params_t, None, n_runs, duration, settling_time, t0)
+        # every clear and the launch go to one stream, ordered after the
+        # caller's work on the current stream
+        st = stream if stream is not None else torch.cuda.current_stream(dev)
+        st.wait_stream(torch.cuda.current_stream(dev))
+        with torch.cuda.stream(st):
+            bufs = s.allocate_outputs(prep, n_runs, dev, tdtype)
+            args = s.make_args(prep, bufs, inits_t, params_t, None, n_runs, duration, settling_time, t0)
         lane, record, tape_entry = self.sizes(prep)
         words = lane // 4
-        ckpt = torch.empty((n_runs * self.max_ckpts * words,), device=dev, dtype=torch.int32)
-        count = torch.zeros((n_runs,), device=dev, dtype=torch.int32)
-        tape = self._tape_buffers(n_runs, tape_entry, dev) if tape_entry > 0 else None
+        with torch.cuda.stream(st):
+            ckpt = torch.empty((n_runs * self.max_ckpts * words,), device=dev, dtype=torch.int32)
+            count = torch.zeros((n_runs,), device=dev, dtype=torch.int32)
+            tape = self._tape_buffers(n_runs, tape_entry, dev) if tape_entry > 0 else None
         adj = _native.AdjointArgs()
         adj.ckpt = ckpt.data_ptr()
         adj.ckpt_count = count.data_ptr()
@@ -103,7 +109,6 @@ class AdjointIntegrator:
         adj.ckpt_every = self.ckpt_every
         adj.max_ckpts = self.max_ckpts
         self._set_tape(adj, tape)
-        st = stream if stream is not None else torch.cuda.current_stream(dev)
         prep["module"].adjoint_launch(args, adj, 0, s.block_size, 0, st.cuda_stream)
         saved = dict(prep=prep, bufs=bufs, inits=inits_t, params=params_t, ckpt=ckpt, count=count, words=words,
                      record=record, tape=tape,
@@ -122,11 +127,16 @@ class AdjointIntegrator:
         grad_state = grad_state.detach().to(device=dev, dtype=tdtype).contiguous()
         if tuple(grad_state.shape) != tuple(bufs["state"].shape):
             raise ValueError(f"grad_state shape {tuple(grad_state.shape)} != state {tuple(bufs['state'].shape)}")
-        seg = torch.empty((self.ckpt_every * n_runs * saved["record"] // 4,), device=dev, dtype=torch.int32)
-        gi = torch.empty((n, n_runs), device=dev, dtype=tdtype)
-        gp = torch.empty((max(npar, 1), n_runs), device=dev, dtype=tdtype)
-        args = s.make_args(prep, bufs, saved["inits"], saved["params"], None, n_runs, saved["duration"],
-                           saved["settling_time"], saved["t0"])  # zeroes the work counter
+        # the work-counter reset and the launch share one stream, ordered
+        # after the caller's work (and the forward launch) on the current one
+        st = stream if stream is not None else torch.cuda.current_stream(dev)
+        st.wait_stream(torch.cuda.current_stream(dev))
+        with torch.cuda.stream(st):
+            seg = torch.empty((self.ckpt_every * n_runs * saved["record"] // 4,), device=dev, dtype=torch.int32)
+            gi = torch.empty((n, n_runs), device=dev, dtype=tdtype)
+            gp = torch.empty((max(npar, 1), n_runs), device=dev, dtype=tdtype)
+            args = s.make_args(prep, bufs, saved["inits"], saved["params"], None, n_runs, saved["duration"],
+                               saved["settling_time"], saved["t0"])  # zeroes the work counter
         adj = _native.AdjointArgs()
         adj.ckpt = saved["ckpt"].data_ptr()
         adj.ckpt_count = saved["count"].data_ptr()
@@ -138,7 +148,6 @@ class AdjointIntegrator:
         adj.ckpt_every = self.ckpt_every
         adj.max_ckpts = self.max_ckpts
         self._set_tape(adj, saved["tape"])
-        st = stream if stream is not None else torch.cuda.current_stream(dev)
         prep["module"].adjoint_launch(args, adj, 1, s.block_size, 0, st.cuda_stream)
         return gi, (gp if npar > 0 else gp[:0])
 

@@ -35,6 +35,7 @@ struct cbx_module {
     size_t tape_bytes;
     bool adj_resolved;
     int n_families;  // families of the heterogeneous kernel (0 without one)
+    int primary;     // 1: context is the device's primary context, 0: it is not, -1: not yet checked
 };
 
 namespace {
@@ -52,6 +53,7 @@ struct DriverApi {
     CBX_DRV(cuCtxGetCurrent)
     CBX_DRV(cuCtxGetDevice)
     CBX_DRV(cuDevicePrimaryCtxRetain)
+    CBX_DRV(cuDevicePrimaryCtxRelease)
     CBX_DRV(cuCtxSetCurrent)
     CBX_DRV(cuModuleLoadData)
     CBX_DRV(cuModuleGetFunction)
@@ -99,7 +101,13 @@ bool load_driver() {
     CBX_SYM(cuGetErrorName)
     CBX_SYM(cuGetErrorString)
 #undef CBX_SYM
-    // versioned entry point: the 64-bit size variant behind cuda.h's macro
+    // versioned entry points behind cuda.h's macros
+    g_drv.cuDevicePrimaryCtxRelease =
+        reinterpret_cast<decltype(g_drv.cuDevicePrimaryCtxRelease)>(dlsym(h, "cuDevicePrimaryCtxRelease_v2"));
+    if (!g_drv.cuDevicePrimaryCtxRelease) {
+        g_drv.failed = true;
+        return false;
+    }
     g_drv.cuModuleGetGlobal = reinterpret_cast<decltype(g_drv.cuModuleGetGlobal)>(dlsym(h, "cuModuleGetGlobal_v2"));
     if (!g_drv.cuModuleGetGlobal) {
         g_drv.failed = true;
@@ -233,6 +241,7 @@ int cbx_module_load(const void* cubin, size_t cubin_size, int device, cbx_module
     cbx_module* m = new cbx_module();
     m->context = ctx;
     m->device = device;
+    m->primary = -1;
     rc = check_cu(g_drv.cuModuleLoadData(&m->module, cubin), "cuModuleLoadData");
     if (rc) {
         delete m;
@@ -304,7 +313,12 @@ int cbx_occupancy(cbx_module* module, int kernel, int block, int* blocks_per_sm)
                     "cuOccupancyMaxActiveBlocksPerMultiprocessor");
 }
 
-int cbx_solve(cbx_module* module, const cbx_solve_args* args, int kernel, int block, int grid, void* stream) {
+}  // extern "C"
+
+namespace {
+// Argument checks of cbx_solve; ``need_counter`` = false for callers that
+// supply the work counter themselves.
+int validate_solve(const cbx_module* module, const cbx_solve_args* args, int kernel, int block, bool need_counter) {
     if (!module || !args) return fail(CBX_ERR_ARGUMENT, "null module or args");
     if (kernel != CBX_KERNEL_PLAIN && kernel != CBX_KERNEL_PERSISTENT && kernel != CBX_KERNEL_WARP)
         return fail(CBX_ERR_ARGUMENT, "unknown kernel kind %d", kernel);
@@ -315,8 +329,17 @@ int cbx_solve(cbx_module* module, const cbx_solve_args* args, int kernel, int bl
         return fail(CBX_ERR_ARGUMENT, "run_stride (%lld) must be >= n_runs (%lld)", args->run_stride,
                     args->n_runs);
     if (!args->inits || !args->status_out) return fail(CBX_ERR_ARGUMENT, "inits and status_out are required");
-    if ((kernel == CBX_KERNEL_PERSISTENT || kernel == CBX_KERNEL_WARP) && !args->work_counter)
+    if (need_counter && (kernel == CBX_KERNEL_PERSISTENT || kernel == CBX_KERNEL_WARP) && !args->work_counter)
         return fail(CBX_ERR_ARGUMENT, "the persistent and warp kernels need a zeroed work_counter");
+    return CBX_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int cbx_solve(cbx_module* module, const cbx_solve_args* args, int kernel, int block, int grid, void* stream) {
+    int vrc = validate_solve(module, args, kernel, block, true);
+    if (vrc) return vrc;
     if (args->n_runs == 0) return CBX_OK;
     CUcontext cur = nullptr;
     g_drv.cuCtxGetCurrent(&cur);
@@ -606,25 +629,37 @@ constexpr int kNoAllocMaxDevices = 64;
 unsigned long long* g_noalloc_addr[kNoAllocMaxDevices] = {};
 std::mutex g_noalloc_mutex;
 
-// Device address of the scratch array on ``device``.  The first call for a
-// device makes that device current, asks the runtime for the address (this
-// loads the library's device code into the device's primary context) and
-// restores the previous device; later calls reuse the address.
+// 0 when the module lives in its device's primary context (the one the
+// CUDA runtime, and so the address of the static array, belongs to).
+int require_primary_context(cbx_module* m) {
+    if (m->primary < 0) {
+        CUdevice dev;
+        int rc = check_cu(g_drv.cuDeviceGet(&dev, m->device), "cuDeviceGet");
+        if (rc) return rc;
+        CUcontext prim = nullptr;
+        rc = check_cu(g_drv.cuDevicePrimaryCtxRetain(&prim, dev), "cuDevicePrimaryCtxRetain");
+        if (rc) return rc;
+        m->primary = prim == m->context ? 1 : 0;
+        g_drv.cuDevicePrimaryCtxRelease(dev);
+    }
+    if (m->primary != 1)
+        return fail(CBX_ERR_ARGUMENT, "cbx_solve_noalloc needs a module loaded in device %d's primary context "
+                    "(the module was loaded while another context was current)", m->device);
+    return CBX_OK;
+}
+
+// Device address of the scratch array on the module's device.  The module's
+// (primary) context must be current.  The first call for a device asks the
+// runtime for the address, which loads this library's device code into the
+// primary context; later calls reuse the address.
 int noalloc_scratch(int device, unsigned long long** out) {
     std::lock_guard<std::mutex> lock(g_noalloc_mutex);
     if (g_noalloc_addr[device]) {
         *out = g_noalloc_addr[device];
         return CBX_OK;
     }
-    int prev = -1;
-    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
-    if (prev != device) {
-        cudaError_t e = cudaSetDevice(device);
-        if (e != cudaSuccess) return fail(CBX_ERR_RUNTIME, "cudaSetDevice(%d): %s", device, cudaGetErrorString(e));
-    }
     void* p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (prev >= 0 && prev != device) cudaSetDevice(prev);
     if (e != cudaSuccess || !p)
         return fail(CBX_ERR_RUNTIME, "cudaGetSymbolAddress of the no-alloc scratch on device %d: %s", device,
                     cudaGetErrorString(e));
@@ -636,19 +671,26 @@ int noalloc_scratch(int device, unsigned long long** out) {
 
 extern "C" int cbx_solve_noalloc(cbx_module* module, const cbx_solve_args* args, int block, int grid,
                                  void* stream) {
-    if (!module || !args) return fail(CBX_ERR_ARGUMENT, "null module or args");
+    // every check that cbx_solve makes comes first: a rejected call leaves
+    // the shared array untouched
+    int rc = validate_solve(module, args, CBX_KERNEL_PERSISTENT, block, false);
+    if (rc) return rc;
     if (module->device < 0 || module->device >= kNoAllocMaxDevices)
         return fail(CBX_ERR_ARGUMENT, "cbx_solve_noalloc supports device ordinals 0-%d, got %d",
                     kNoAllocMaxDevices - 1, module->device);
-    unsigned long long* scratch = nullptr;
-    int rc = noalloc_scratch(module->device, &scratch);
+    if (!load_driver()) return fail(CBX_ERR_NO_DEVICE, "CUDA driver library is not available");
+    rc = require_primary_context(module);
     if (rc) return rc;
+    if (args->n_runs == 0) return CBX_OK;
     CUcontext cur = nullptr;
     g_drv.cuCtxGetCurrent(&cur);
     if (cur != module->context) {
         rc = check_cu(g_drv.cuCtxSetCurrent(module->context), "cuCtxSetCurrent");
         if (rc) return rc;
     }
+    unsigned long long* scratch = nullptr;
+    rc = noalloc_scratch(module->device, &scratch);
+    if (rc) return rc;
     cbx_solve_args local = *args;
     local.work_counter = scratch;
     const bool scratch_totals = local.totals == nullptr;

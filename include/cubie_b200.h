@@ -154,13 +154,16 @@ int cbx_adjoint_launch(cbx_module* module, const cbx_solve_args* args, const cbx
  * before the launch; the array keeps the last call's values afterwards.
  * Calls that overlap on the GPU (on different streams, or from several
  * threads) share the array and race: serialise them.  Rejects device
- * ordinals of 64 and above.  Calls no cudaMalloc or cudaFree.
+ * ordinals of 64 and above, and modules loaded while a context other than
+ * the device's primary context was current (the array's address belongs to
+ * the primary context).  Every argument check comes before the clear, so a
+ * rejected call touches nothing on the device.  Calls no cudaMalloc or
+ * cudaFree.
  *
  * The first call on a device looks up the array's device address with
- * cudaGetSymbolAddress (making that device current for the lookup and then
- * restoring the previous device), which loads this library's device code
- * into the device's primary context: make that first call before any
- * stream capture. */
+ * cudaGetSymbolAddress, with the module's (primary) context current, which
+ * loads this library's device code into that context: make that first
+ * call before any stream capture. */
 int cbx_solve_noalloc(cbx_module* module, const cbx_solve_args* args, int block, int grid,
                       void* stream);
 

@@ -28,6 +28,58 @@ FHN = dict(
 )
 
 
+def hh_cable_equations(nc):
+    """An nc-compartment Hodgkin-Huxley cable: states V, m, h, n per
+    compartment (grouped by variable), parameters gNa, gK, gc, driver I
+    injected into compartment 0, sealed ends."""
+    V = [f"V{j:02d}" for j in range(nc)]
+    eqs = []
+    for j in range(nc):
+        v, m, h, n = V[j], f"m{j:02d}", f"h{j:02d}", f"n{j:02d}"
+        left = V[j - 1] if j > 0 else v
+        right = V[j + 1] if j < nc - 1 else v
+        inj = "I + " if j == 0 else ""
+        eqs.append(f"d{v} = {inj}gc * ({left} - 2 * {v} + {right}) - gNa * {m}**3 * {h} * ({v} - 50.0)"
+                   f" - gK * {n}**4 * ({v} + 77.0) - 0.3 * ({v} + 54.4)")
+    for j in range(nc):
+        v, m = V[j], f"m{j:02d}"
+        eqs.append(f"d{m} = 0.1 * ({v} + 40.0) / (1 - exp(-({v} + 40.0) / 10.0)) * (1 - {m})"
+                   f" - 4.0 * exp(-({v} + 65.0) / 18.0) * {m}")
+    for j in range(nc):
+        v, h = V[j], f"h{j:02d}"
+        eqs.append(f"d{h} = 0.07 * exp(-({v} + 65.0) / 20.0) * (1 - {h}) - 1.0 / (1 + exp(-({v} + 35.0) / 10.0)) * {h}")
+    for j in range(nc):
+        v, n = V[j], f"n{j:02d}"
+        eqs.append(f"d{n} = 0.01 * ({v} + 55.0) / (1 - exp(-({v} + 55.0) / 10.0)) * (1 - {n})"
+                   f" - 0.125 * exp(-({v} + 65.0) / 80.0) * {n}")
+    states = [*V, *(f"m{j:02d}" for j in range(nc)), *(f"h{j:02d}" for j in range(nc)),
+              *(f"n{j:02d}" for j in range(nc))]
+    return dict(equations=eqs, states=states, parameters=["gNa", "gK", "gc"], constants={}, drivers=["I"])
+
+
+HH64 = hh_cable_equations(64)
+
+
+def hh_inputs(n, seed, nc=64):
+    """Resting cable (V -65, m 0.05, h 0.6, n 0.32) with small seeded
+    perturbations; gNa ~ U[80,160], gK ~ U[20,50], gc ~ U[0.1,1]."""
+    rng = np.random.default_rng(seed)
+    rest = np.repeat([-65.0, 0.05, 0.6, 0.32], nc)[:, None]
+    scale = np.repeat([0.5, 0.005, 0.005, 0.005], nc)[:, None]
+    x0 = rest + scale * rng.normal(0.0, 1.0, (4 * nc, n))
+    p = np.stack([rng.uniform(80, 160, n), rng.uniform(20, 50, n), rng.uniform(0.1, 1.0, n)])
+    return x0, p
+
+
+def vdp_manifold_inputs(x0s, mus):
+    """Van der Pol runs started at x0 on y = 0: with x0 slightly above 1 the
+    run reaches the fold of the slow manifold within
+    mu (x0^2 / 2 - ln x0 - 1/2) time units and makes one fast relaxation
+    transition to x ~ -2 early in the window."""
+    x0 = np.stack([np.asarray(x0s, dtype=float), np.zeros(len(x0s))])
+    return x0, np.asarray(mus, dtype=float)[None, :]
+
+
 def lorenz_inputs(n, seed):
     rng = np.random.default_rng(seed)
     rho = rng.uniform(20.0, 35.0, n)
@@ -214,6 +266,37 @@ CASES.update({
 })
 
 
+# Stiff Van der Pol at the headline's stiffness (mu up to 1000) over a
+# window with one relaxation transition per run, and the 64-compartment
+# (256-state) Hodgkin-Huxley cable with its step current over a window that
+# holds the first spike.  ``engine`` holds settings of this engine only
+# (the fixture generator does not pass them to the reference).
+_MU = ("vdp_manifold", [1.4, 1.2, 1.1], [100.0, 300.0, 1000.0])
+_HH_DRV = dict(seed=0, n_samples=1000, period=0.01, t0=0.0, order=3, wrap=False, boundary_condition="clamped",
+               step=(10.0, 5.0))
+CASES.update({
+    "vdp_stiff_ros3p_f32": dict(system=VDP, algorithm="ros3p", precision="float32", inputs=_MU, duration=20.0,
+                                kwargs=dict(rtol=1e-6, atol=1e-6, save_every=2.0, output_types=_ITS)),
+    "vdp_stiff_ros3p_f64": dict(system=VDP, algorithm="ros3p", precision="float64", inputs=_MU, duration=20.0,
+                                kwargs=dict(rtol=1e-6, atol=1e-6, save_every=2.0, linear_correction_type="bicgstab",
+                                            output_types=_ITS)),
+    "vdp_stiff_radau_f32": dict(system=VDP, algorithm="radau", precision="float32", inputs=_MU, duration=20.0,
+                                kwargs=dict(rtol=1e-6, atol=1e-6, save_every=2.0, output_types=_ITS)),
+    "vdp_stiff_radau_f64": dict(system=VDP, algorithm="radau", precision="float64", inputs=_MU, duration=20.0,
+                                kwargs=dict(rtol=1e-6, atol=1e-6, save_every=2.0, linear_correction_type="bicgstab",
+                                            output_types=_ITS)),
+    "hh64_dirk3_bicgstab_f32": dict(system=HH64, algorithm="l_stable_dirk_3", precision="float32",
+                                    inputs=("hh", 2, 60), duration=4.0, drivers=_HH_DRV,
+                                    engine=dict(layout="warp"),
+                                    kwargs=dict(dt=0.025, rtol=1e-4, atol=1e-4, linear_correction_type="bicgstab",
+                                                save_every=0.5, summarise_every=4.0, sample_summaries_every=0.05,
+                                                summarise_variables=[f"V{j:02d}" for j in range(64)],
+                                                saved_state_indices=list(range(64)),
+                                                output_types=["state", "time", "iteration_counters", "mean",
+                                                              "max"])),
+})
+
+
 def case_inputs(case):
     kind = case["inputs"][0]
     if kind == "lorenz":
@@ -224,6 +307,10 @@ def case_inputs(case):
         return fhn_inputs(case["inputs"][1], case["inputs"][2])
     if kind == "driven":
         return driven_inputs(case["inputs"][1], case["inputs"][2])
+    if kind == "hh":
+        return hh_inputs(case["inputs"][1], case["inputs"][2])
+    if kind == "vdp_manifold":
+        return vdp_manifold_inputs(case["inputs"][1], case["inputs"][2])
     raise KeyError(kind)
 
 
@@ -236,6 +323,13 @@ def case_drivers(case):
     rng = np.random.default_rng(spec["seed"])
     out = {"driver_sample_period": spec["period"], "t0": spec["t0"], "order": spec["order"],
            "wrap": spec["wrap"], "boundary_condition": spec["boundary_condition"]}
+    if spec.get("step") is not None:
+        # a step current: ``level`` before ``t_off``, 0 after
+        level, t_off = spec["step"]
+        t = spec["t0"] + spec["period"] * np.arange(spec["n_samples"])
+        for name in case["system"]["drivers"]:
+            out[name] = np.where(t < t_off, level, 0.0)
+        return out
     for name in case["system"]["drivers"]:
         samples = rng.uniform(-1.0, 1.0, spec["n_samples"])
         if spec["boundary_condition"] == "periodic":

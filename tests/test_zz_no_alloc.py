@@ -56,10 +56,16 @@ def test_noalloc_matches_cbx_solve_on_two_calls(cuda_device):
         args.work_counter = None
         # first call: totals in the scratch array; second: in a caller buffer
         args.totals = None if call == 0 else out["totals"].data_ptr()
+        torch.cuda.synchronize(dev)
+        free_before = torch.cuda.mem_get_info(dev)[0]
         rc = L.cbx_solve_noalloc(prep["module"]._handle, ctypes.byref(args), solver.block_size, 0,
                                  ctypes.c_void_p(stream.cuda_stream))
         assert rc == 0, L.cbx_last_error().decode()
         torch.cuda.synchronize(dev)
+        if call == 1:
+            # the defining property: after the first call on the device has
+            # looked the array up, a call takes no device memory
+            assert torch.cuda.mem_get_info(dev)[0] == free_before
 
         status = out["status"].cpu().numpy()
         np.testing.assert_array_equal(status, ref["status"].cpu().numpy())
