@@ -529,6 +529,11 @@ class Settings:
     output_types: Sequence[str] = ("state",)
     dense_prediction: bool = True
     max_steps: int = 0
+    # variable selection (output_config.py: saved_state_indices,
+    # summarised_state_indices; summarise_variables by state name)
+    saved_state_indices: Optional[Sequence[int]] = None
+    summarised_state_indices: Optional[Sequence[int]] = None
+    summarise_variables: Optional[Sequence[str]] = None
 
 
 def integrate(system: OracleSystem, algorithm: str, inits: np.ndarray, params: np.ndarray,
@@ -1358,5 +1363,14 @@ def integrate(system: OracleSystem, algorithm: str, inits: np.ndarray, params: n
                 summ_idx = summ_idx + sv
         if iteration > 10_000_000:
             raise RuntimeError("oracle loop did not terminate")
+    if S.saved_state_indices is not None and save_state:
+        keep = list(S.saved_state_indices) + ([width - 1] if save_time else [])
+        out_state = out_state[:, keep, :]
+    summ_sel = S.summarised_state_indices
+    if S.summarise_variables is not None:
+        summ_sel = [system.states.index(v) for v in S.summarise_variables]
+    if summ_sel is not None and summarise:
+        rows = out_summ.shape[0]
+        out_summ = out_summ.reshape(rows, n, out_w, B)[:, list(summ_sel)].reshape(rows, len(summ_sel) * out_w, B)
     return dict(state=out_state, iteration_counters=out_cnt, state_summaries=out_summ,
                 status=status.astype(np.int32), n_save=n_save, n_summ=n_summ)

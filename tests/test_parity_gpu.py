@@ -25,6 +25,7 @@ def _solve(case, kernel="plain", **extra):
     system = build_case_system(case)
     inits, params = case_inputs(case)
     kw = dict(case["kwargs"])
+    kw.update(case.get("engine", {}))
     kw.update(extra)
     solver = Solver(system, algorithm=case["algorithm"], kernel=kernel, **kw)
     prec = np.dtype(case["precision"]).type
