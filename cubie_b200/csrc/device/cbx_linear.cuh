@@ -80,6 +80,14 @@ __device__ __forceinline__ int solve_mr(const Op& op, typename Cfg::R* rhs,
     return converged ? SUCCESS : MAX_LINEAR_ITERATIONS_EXCEEDED;
 }
 
+// Operators may keep BiCGSTAB's shadow residual in shared memory
+// (``SHADOW_SHARED``, with ``shadow()`` and ``slot(i)`` giving its storage);
+// by default it is a register array.
+template <class Op, class = void> struct ShadowShared { static constexpr bool value = false; };
+template <class Op> struct ShadowShared<Op, decltype(void(Op::SHADOW_SHARED))> {
+    static constexpr bool value = Op::SHADOW_SHARED;
+};
+
 template <class R> __device__ __forceinline__ R clampd(R v, R lim) {
     v = (v > lim) ? lim : v;
     return (v < -lim) ? -lim : v;
@@ -99,7 +107,14 @@ __device__ __forceinline__ int solve_bicgstab(const Op& op, typename Cfg::R* rhs
     constexpr bool F32 = sizeof(R) == 4;
     const R tiny = F32 ? R(1e-30) : R(1e-200);
     const R lim = F32 ? R(1e16) : R(1e150);
-    R r0[K], p[K], v[K], tmp[K], sh[K];
+    constexpr bool SHS = ShadowShared<Op>::value;
+    R r0[SHS ? 1 : K], p[K], v[K], tmp[K], sh[K];
+    R* r0s = nullptr;
+    if constexpr (SHS) r0s = op.shadow();
+    auto shadow_at = [&](int i) -> R {
+        if constexpr (SHS) return r0s[op.slot(i)];
+        else return r0[i];
+    };
 
     const C rhs_norm2 = op.wnorm2(rhs);
     const C tol = C(Cfg::KRYLOV_FLOOR) + C(Cfg::KRYLOV_REDUCTION) * sqrt_t(rhs_norm2);
@@ -111,7 +126,8 @@ __device__ __forceinline__ int solve_bicgstab(const Op& op, typename Cfg::R* rhs
         const R ax = clampd(tmp[i], lim);
         const R ri = rhs[i] - ax;
         rhs[i] = ri;
-        r0[i] = ri;
+        if constexpr (SHS) r0s[op.slot(i)] = ri;
+        else r0[i] = ri;
         p[i] = clampd(ri, lim);
         R sq = ri * ri;
         sq = (sq > lim) ? lim : sq;
@@ -139,7 +155,7 @@ __device__ __forceinline__ int solve_bicgstab(const Op& op, typename Cfg::R* rhs
 #pragma unroll
         for (int i = 0; i < K; ++i) {
             v[i] = clampd(v[i], lim);
-            dot_r0v += clampd(r0[i] * v[i], lim);
+            dot_r0v += clampd(shadow_at(i) * v[i], lim);
         }
         dot_r0v = op.reduce(dot_r0v);
         const bool alpha_overflow = absv(rho_prev) > absv(dot_r0v) * lim;
@@ -186,7 +202,7 @@ __device__ __forceinline__ int solve_bicgstab(const Op& op, typename Cfg::R* rhs
         converged = converged || (acc <= tol2);
         R rho_new = R(0);
 #pragma unroll
-        for (int i = 0; i < K; ++i) rho_new += clampd(r0[i] * rhs[i], lim);
+        for (int i = 0; i < K; ++i) rho_new += clampd(shadow_at(i) * rhs[i], lim);
         rho_new = op.reduce(rho_new);
         const bool rho_bad = absv(rho_new) < tiny;
         const bool omega_bad = absv(omega) < tiny;

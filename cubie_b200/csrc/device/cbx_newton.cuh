@@ -135,6 +135,11 @@ struct CoupledOp {
     static constexpr int KT = K;
 };
 
+// Problems whose residual and linearisation share work at one iterate
+// (``FUSED``) provide residual_linearize(u, out) in place of the two calls.
+template <class P, class = void> struct HasFused { static constexpr bool value = false; };
+template <class P> struct HasFused<P, decltype(void(P::FUSED))> { static constexpr bool value = P::FUSED; };
+
 // Damped Newton iteration with NLNewton-style acceptance
 // (newton_krylov.py:340-517): contraction estimate theta carried between
 // solves, acceptance eta*||dz|| < kappa (kappa = 0.01), a first-iteration
@@ -164,13 +169,14 @@ __device__ __forceinline__ int newton_solve(Prob& prob, typename Cfg::R* u, type
     R res[K], delta[K];
     for (int it = 0; it < Cfg::NEWTON_MAX_ITERS; ++it) {
         if (converged || failed) break;
-        prob.residual(u, res);
+        if constexpr (HasFused<Prob>::value) prob.residual_linearize(u, res);
+        else prob.residual(u, res);
 #pragma unroll
         for (int i = 0; i < K; ++i) {
             res[i] = -res[i];
             delta[i] = R(0);
         }
-        prob.linearize(u);
+        if constexpr (!HasFused<Prob>::value) prob.linearize(u);
         int kit = 0;
         const int lin = linear_solve<Cfg>(prob.op(), res, delta, kit);
         total_k += kit;

@@ -34,14 +34,28 @@ __device__ __forceinline__ T warp_sum(T v) {
     return __shfl_sync(kWarpFull, v, 0);
 }
 
+// Per-warp shared memory.  With a cached Jacobian (WSys::NNZ > 0) the
+// linearisation stores J's nonzero coefficients in ``jac`` and every J v
+// reads them back; otherwise J v is re-derived from the linearisation
+// point ``ylin``.  With Cfg::SHARED_SCRATCH the stage solve's base state,
+// the step's start state and BiCGSTAB's shadow residual live here too
+// ("shared" placement); otherwise they stay in the calling thread's
+// registers or local memory ("local" placement).
 template <class Cfg>
 struct WarpMem {
     using R = typename Cfg::R;
     static constexpr int N = Cfg::N;
+    static constexpr bool CACHED = Cfg::WSys::NNZ > 0;
+    static constexpr int SH = Cfg::SHARED_SCRATCH ? N : 1;
     R ys[N];                              // state of a right-hand-side evaluation
-    R ylin[N];                            // linearisation point of the Newton operator
     R vs[N];                              // operand of J v
     R out[N];                             // class outputs
+    R kw[N];                              // Krylov weights 1 / tol_i of the current stage solve
+    R jac[CACHED ? Cfg::WSys::NNZ : 1];   // cached Jacobian coefficients
+    R ylin[CACHED ? 1 : N];               // linearisation point (matrix-free J v)
+    R sbase[SH];                          // stage base state (shared placement)
+    R sstart[SH];                         // step start state (shared placement)
+    R r0[Cfg::SHARED_SCRATCH ? 32 * ((N + 31) / 32) : 1];  // BiCGSTAB shadow residual (shared placement)
     R p[Cfg::NP > 0 ? Cfg::NP : 1];
     R d[Cfg::ND > 0 ? Cfg::ND : 1];       // drivers of the evaluation
     R dlin[Cfg::ND > 0 ? Cfg::ND : 1];    // drivers at the linearisation point
@@ -52,6 +66,7 @@ struct WarpCtx {
     using R = typename Cfg::R;
     using C = typename Cfg::C;
     static constexpr int N = Cfg::N, ND = Cfg::ND, L = (Cfg::N + 31) / 32;
+    static constexpr bool CACHED = WarpMem<Cfg>::CACHED;
     WarpMem<Cfg>* m;
     int lane;
     const R* coeffs;
@@ -84,16 +99,42 @@ struct WarpCtx {
         __syncwarp();
     }
     __device__ __forceinline__ void linearize(const R* Yloc, R t, const R* drv) {
-        put(m->ylin, Yloc);
-        put_drivers(m->dlin, drv);
-        tlin = t;
-        __syncwarp();
+        if constexpr (CACHED) {
+            R scratch[L];
+            rhs_linearize(Yloc, t, drv, scratch);
+        } else {
+            put(m->ylin, Yloc);
+            put_drivers(m->dlin, drv);
+            tlin = t;
+            __syncwarp();
+        }
+    }
+    // f(t, Y) and the linearisation at Y in one pass: with a cached
+    // Jacobian, f and J's coefficients share their subexpressions (the
+    // exponentials of a gating rate appear in both).
+    __device__ __forceinline__ void rhs_linearize(const R* Yloc, R t, const R* drv, R* floc) {
+        if constexpr (CACHED) {
+            put(m->ys, Yloc);
+            put_drivers(m->d, drv);
+            __syncwarp();
+            Cfg::WSys::template fj_lanes<R>(m->ys, m->p, m->d, t, m->out, m->jac, lane);
+            __syncwarp();
+            get(m->out, floc);
+            __syncwarp();
+        } else {
+            rhs(Yloc, t, drv, floc);
+            linearize(Yloc, t, drv);
+        }
     }
     // J(y_lin) v: v and the result local.
     __device__ __forceinline__ void jmv(const R* vloc, R* outloc) {
         put(m->vs, vloc);
         __syncwarp();
-        Cfg::WSys::template jmv_lanes<R>(m->ylin, m->vs, m->p, m->dlin, tlin, m->out, lane);
+        if constexpr (CACHED) {
+            Cfg::WSys::template jmv_cached<R>(m->vs, m->jac, m->out, lane);
+        } else {
+            Cfg::WSys::template jmv_lanes<R>(m->ylin, m->vs, m->p, m->dlin, tlin, m->out, lane);
+        }
         __syncwarp();
         get(m->out, outloc);
         __syncwarp();
@@ -101,15 +142,18 @@ struct WarpCtx {
 };
 
 // v - s J(y_lin) v over the warp, with the truncated Neumann preconditioner.
+// Its weighted norm reads the Krylov weights 1 / tol_i that the stage solve
+// formed once from the stage base (the base is fixed for the whole solve),
+// in the working precision.
 template <class Cfg>
 struct WarpStageOp {
     using R = typename Cfg::R;
     using C = typename Cfg::C;
     static constexpr int K = WarpCtx<Cfg>::L;
     static constexpr int KT = Cfg::N;
+    static constexpr bool SHADOW_SHARED = Cfg::SHARED_SCRATCH;
     WarpCtx<Cfg>* w;
     R s;
-    const R* ref;
     __device__ __forceinline__ void apply(const R* v, R* out) const {
         R jv[K];
         w->jmv(v, jv);
@@ -128,38 +172,53 @@ struct WarpStageOp {
     }
     __device__ __forceinline__ C tol(int i) const {
         const int c = w->lane + 32 * i;
-        return c < Cfg::N ? krylov_tol<Cfg>(c, ref[i], w->tol_scale) : C(1);
+        return c < Cfg::N ? C(R(1) / w->m->kw[c]) : C(1);
     }
     __device__ __forceinline__ C wnorm2(const R* v) const {
-        C s2 = C(0);
+        R s2 = R(0);
 #pragma unroll
         for (int i = 0; i < K; ++i) {
             if (w->valid(i)) {
-                const C ratio = C(absv(v[i])) / tol(i);
+                const R ratio = v[i] * w->m->kw[w->lane + 32 * i];
                 s2 += ratio * ratio;
             }
         }
-        return warp_sum(s2) * (C(1) / C(Cfg::N));
+        return C(warp_sum(s2) * (R(1) / R(Cfg::N)));
     }
+    // BiCGSTAB's shadow residual in shared memory (shared placement)
+    __device__ __forceinline__ R* shadow() const { return w->m->r0; }
+    __device__ __forceinline__ int slot(int i) const { return w->lane + 32 * i; }
     template <class T>
     __device__ __forceinline__ T reduce(T partial) const { return warp_sum(partial); }
 };
 
-// z = h f(t, base + a z) solved by Newton over the warp (DirkProblem).
+// z = h f(t, base + a z) solved by Newton over the warp (DirkProblem).  The
+// base and step-start states are read through ``b(k)`` / ``y0(k)``: from
+// shared memory with the shared placement, from the caller's arrays
+// otherwise.
 template <class Cfg>
 struct WarpDirkProblem {
     using R = typename Cfg::R;
     using C = typename Cfg::C;
     static constexpr int K = WarpCtx<Cfg>::L;
+    static constexpr bool FUSED = true;
     WarpCtx<Cfg>* w;
     const R* base;
     const R* step_start;
     const R* drv;
     R t, h, a;
+    __device__ __forceinline__ R b(int k) const {
+        if constexpr (Cfg::SHARED_SCRATCH) return w->valid(k) ? w->m->sbase[w->lane + 32 * k] : R(0);
+        else return base[k];
+    }
+    __device__ __forceinline__ R y0(int k) const {
+        if constexpr (Cfg::SHARED_SCRATCH) return w->valid(k) ? w->m->sstart[w->lane + 32 * k] : R(0);
+        else return step_start[k];
+    }
     __device__ __forceinline__ void residual(const R* z, R* out) const {
         R Y[K], f[K];
 #pragma unroll
-        for (int k = 0; k < K; ++k) Y[k] = base[k] + a * z[k];
+        for (int k = 0; k < K; ++k) Y[k] = b(k) + a * z[k];
         w->rhs(Y, t, drv, f);
 #pragma unroll
         for (int k = 0; k < K; ++k) out[k] = w->valid(k) ? z[k] - h * f[k] : R(0);
@@ -167,18 +226,39 @@ struct WarpDirkProblem {
     __device__ __forceinline__ void linearize(const R* z) {
         R Y[K];
 #pragma unroll
-        for (int k = 0; k < K; ++k) Y[k] = base[k] + a * z[k];
+        for (int k = 0; k < K; ++k) Y[k] = b(k) + a * z[k];
         w->linearize(Y, t, drv);
     }
-    __device__ __forceinline__ WarpStageOp<Cfg> op() const { return WarpStageOp<Cfg>{w, a * h, base}; }
+    // residual and linearisation at the same iterate (the Newton loop
+    // evaluates both at every iteration)
+    __device__ __forceinline__ void residual_linearize(const R* z, R* out) {
+        R Y[K], f[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k) Y[k] = b(k) + a * z[k];
+        w->rhs_linearize(Y, t, drv, f);
+#pragma unroll
+        for (int k = 0; k < K; ++k) out[k] = w->valid(k) ? z[k] - h * f[k] : R(0);
+    }
+    __device__ __forceinline__ WarpStageOp<Cfg> op() const { return WarpStageOp<Cfg>{w, a * h}; }
+    // Krylov weights 1 / max(katol + krtol * scale * |base|, 1e-16), once per
+    // stage solve
+    __device__ __forceinline__ void form_weights() const {
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            if (!w->valid(k)) continue;
+            const int c = w->lane + 32 * k;
+            w->m->kw[c] = R(C(1) / krylov_tol<Cfg>(c, b(k), w->tol_scale));
+        }
+        __syncwarp();
+    }
     __device__ __forceinline__ C corr_norm2(const R* delta, const R* z) const {
         C nrm2 = C(0);
 #pragma unroll
         for (int k = 0; k < K; ++k) {
             if (!w->valid(k)) continue;
             const int c = w->lane + 32 * k;
-            const R sv = base[k] + a * z[k];
-            const R ref = pymax(absv(sv), absv(step_start[k]));
+            const R sv = b(k) + a * z[k];
+            const R ref = pymax(absv(sv), absv(y0(k)));
             C tol = C(Cfg::natol(c)) + C(Cfg::nrtol(c)) * w->tol_scale * C(ref);
             tol = pymax(tol, C(1e-16));
             const C ratio = C(delta[k]) / tol;
@@ -216,9 +296,10 @@ struct WarpDirkStep {
     // runs 24 % faster.  Moving the operator and norm helpers out of line
     // as well (98 KB) was slower again: their calls pass the per-lane
     // vectors through the stack.
-    static __device__ CBX_NOINLINE int stage_solve(WarpCtx<Cfg>& w, R* base, const R* y, const R* drv_stage,
+    static __device__ CBX_NOINLINE int stage_solve(WarpCtx<Cfg>& w, const R* base, const R* y, const R* drv_stage,
                                                       R stage_time, R dt, R a, Persist& ps, Iters& its) {
         WarpDirkProblem<Cfg> prob{&w, base, y, drv_stage, stage_time, dt, a};
+        prob.form_weights();
         int ni = 0, ki = 0;
         const int st = newton_solve<Cfg>(prob, ps.z, ps.theta, ni, ki);
         its.nit = ni;
@@ -227,12 +308,26 @@ struct WarpDirkStep {
         its.kit_all += ki;
         return st;
     }
+    // With the shared placement the stage base goes to shared memory before
+    // the solve and no address of a per-lane array crosses the call, so those
+    // arrays stay in registers.
+    static __device__ __forceinline__ int solve_stage(WarpCtx<Cfg>& w, const R* base, const R* y,
+                                                      const R* drv_stage, R stage_time, R dt, R a, Persist& ps,
+                                                      Iters& its) {
+        if constexpr (Cfg::SHARED_SCRATCH) {
+            w.put(w.m->sbase, base);
+            return stage_solve(w, nullptr, nullptr, drv_stage, stage_time, dt, a, ps, its);
+        } else {
+            return stage_solve(w, base, y, drv_stage, stage_time, dt, a, ps, its);
+        }
+    }
     static __device__ __forceinline__ int step(WarpCtx<Cfg>& w, const R* y, R* ynew, R* delta, R* err,
                                                const R* drv, R* drv_new, R dt, R t, bool first_step,
                                                bool prev_accepted, Persist& ps, Iters& its) {
         its = Iters{};
         int status = SUCCESS;
         const bool use_cached = Tab::FSAL && (S > 1) && !first_step && prev_accepted;
+        if constexpr (Cfg::SHARED_SCRATCH) w.put(w.m->sstart, y);
         R base[L], outacc[L], erracc[L];
         R acc[(S > 1 ? S - 1 : 1)][L];
         R drv_stage[ND > 0 ? ND : 1];
@@ -257,7 +352,7 @@ struct WarpDirkStep {
                 }
             }
             if (Tab::a(0, 0) != 0.0) {
-                status |= stage_solve(w, base, y, drv_stage, stage_time, dt, R(Tab::a(0, 0)), ps, its);
+                status |= solve_stage(w, base, y, drv_stage, stage_time, dt, R(Tab::a(0, 0)), ps, its);
 #pragma unroll
                 for (int i = 0; i < L; ++i) base[i] += R(Tab::a(0, 0)) * ps.z[i];
             }
@@ -299,7 +394,7 @@ struct WarpDirkStep {
 #pragma unroll
                     for (int i = 0; i < L; ++i) ps.z[i] = dt * ps.rhs[i];
                 }
-                status |= stage_solve(w, base, y, drv_stage, stage_time, dt, R(Tab::a(stage, stage)), ps, its);
+                status |= solve_stage(w, base, y, drv_stage, stage_time, dt, R(Tab::a(stage, stage)), ps, its);
 #pragma unroll
                 for (int i = 0; i < L; ++i) {
                     base[i] += R(Tab::a(stage, stage)) * ps.z[i];

@@ -102,6 +102,10 @@ class KernelSpec:
     adjoint: bool = False
     # "thread": one run per thread; "warp": one run per warp (large systems)
     layout: str = "thread"
+    # where the warp layout keeps its stage-solve scratch vectors (stage
+    # base, step start, BiCGSTAB shadow residual): "shared" memory of the
+    # warp, or "local" (the lane's registers, spilling to local memory)
+    scratch_placement: str = "shared"
 
     @property
     def adaptive(self) -> bool:
@@ -254,14 +258,35 @@ def family_block(system: SymbolicODE, spec: KernelSpec, gen: GeneratedSystem, ns
         lines.append(warp_source)
     tol_arrays = [("atol", spec.atol), ("rtol", spec.rtol), ("katol", katol), ("krtol", krtol), ("natol", natol),
                   ("nrtol", nrtol)]
+    # A tolerance that is the same for every component becomes a literal;
+    # otherwise a table: __constant__ where each lane reads one entry at a
+    # time (thread layout), global memory where the lanes of a warp read
+    # different entries at once (warp layout; the constant cache would
+    # serialise those reads).
+    accessors = []
     for name, vals in tol_arrays:
-        lines.append(_const_array(f"cbx_{name}", ctype, [castp(v) for v in np.broadcast_to(vals, (n,))]))
+        cv = [castp(v) for v in np.broadcast_to(vals, (n,))]
+        if all(v == cv[0] for v in cv):
+            accessors.append(f"    static __device__ __forceinline__ C {name}(int) {{ return C({_lit(cv[0])}); }}")
+            continue
+        decl = _const_array(f"cbx_{name}", ctype, cv)
+        if warp_source is not None:
+            decl = "__device__ const " + decl[len("__constant__ "):]
+        lines.append(decl)
+        accessors.append(f"    static __device__ __forceinline__ C {name}(int i) {{ return cbx_{name}[i]; }}")
     idx_fns = []
     for fname, vals in (("saved_state", spec.saved_state_indices), ("saved_obs", spec.saved_observable_indices),
                         ("summ_state", spec.summarised_state_indices), ("summ_obs", spec.summarised_observable_indices)):
         vv = [int(v) for v in vals] or [0]
-        idx_fns.append(f"    static __host__ __device__ constexpr int {fname}(int k) {{ constexpr int v[{len(vv)}] = "
-                       f"{{{', '.join(str(v) for v in vv)}}}; return v[k]; }}")
+        step = vv[1] - vv[0] if len(vv) > 1 else 0
+        if all(v == vv[0] + step * k for k, v in enumerate(vv)):
+            # an affine selection (the common ranges) needs no table, which a
+            # lane-dependent index would otherwise rebuild in local memory
+            idx_fns.append(f"    static __host__ __device__ constexpr int {fname}(int k) {{ "
+                           f"return {vv[0]} + {step} * k; }}")
+        else:
+            idx_fns.append(f"    static __host__ __device__ constexpr int {fname}(int k) {{ constexpr int v[{len(vv)}] = "
+                           f"{{{', '.join(str(v) for v in vv)}}}; return v[k]; }}")
     lines.append("struct Idx {\n" + "\n".join(idx_fns) + "\n};")
     lines.append(tableau_struct(tab, spec.precision, dense))
     save_every = castp(spec.save_every) if spec.save_every is not None else 0.0
@@ -324,9 +349,11 @@ def family_block(system: SymbolicODE, spec: KernelSpec, gen: GeneratedSystem, ns
         f"    static constexpr bool DRV_WRAP = {str(spec.driver_wrap).lower()};",
         f"    static constexpr int BLOCK = {int(spec.block_size)};",
         f"    static constexpr int MIN_BLOCKS = {max(int(spec.min_blocks_per_sm), 1)};",
+        f"    static constexpr bool SHARED_SCRATCH = "
+        f"{str(spec.layout == 'warp' and spec.scratch_placement == 'shared').lower()};",
         f"    using Step = {STEP_TYPES[tab.kind]};",
         *([f"    using WSys = {ns}::WarpSystem;"] if warp_source is not None else []),
-        *[f"    static __device__ __forceinline__ C {name}(int i) {{ return cbx_{name}[i]; }}" for name, _ in tol_arrays],
+        *accessors,
         "};",
     ]
     lines.append("\n".join(cfg))

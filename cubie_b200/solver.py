@@ -57,7 +57,7 @@ LOOP_KEYS = {"save_every", "summarise_every", "sample_summaries_every"}
 DIRECT_MAX_WIDTH = 16
 EXECUTION_KEYS = {"mixed_precision", "kernel", "block_size", "min_blocks_per_sm", "max_steps", "device", "fast_math",
                   "precision", "adjoint", "layout", "schedule", "mem_proportion", "host_spill_threshold",
-                  "spill_dir", "max_chunk_runs"}
+                  "spill_dir", "max_chunk_runs", "scratch_placement"}
 IGNORED_KEYS = {"memory_settings", "cache", "auto_memory", "lineinfo", "time_logging_level",
                 "profileCUDA", "cache_settings"}
 RENAMED = {"dt_save": "save_every", "dt_summarise": "summarise_every",
@@ -146,6 +146,13 @@ class Solver:
         if layout not in ("thread", "warp"):
             raise ValueError("layout must be 'thread', 'warp' or 'auto'")
         self.layout = layout
+        # warp layout: stage-solve scratch vectors in "shared" memory or
+        # "local" (registers / local memory); "auto" lets the autotuner pick
+        sp_ = str(execution.get("scratch_placement", "shared"))
+        if sp_ not in ("shared", "local", "auto"):
+            raise ValueError("scratch_placement must be 'shared', 'local' or 'auto'")
+        self.placement_pending = sp_ == "auto"
+        self.scratch_placement = "shared" if sp_ == "auto" else sp_
         # claim order of persistent launches: "auto" / "longest_first" sort
         # runs by decreasing per-run horizon when horizons are given
         self.schedule = str(execution.get("schedule", "auto"))
@@ -402,6 +409,7 @@ class Solver:
             mixed_precision=self.mixed_precision, block_size=self.block_size,
             min_blocks_per_sm=self.min_blocks_per_sm, adjoint=self.adjoint, layout=self.layout,
             dense_prediction=None if self.attempt_dense_prediction else False,
+            scratch_placement=self.scratch_placement,
         )
 
     def _generate(self, spec: KernelSpec):

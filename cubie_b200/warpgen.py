@@ -110,6 +110,13 @@ class WarpSystemCode:
     n_classes_f: int
     n_classes_jv: int
     flops: Dict[str, FlopCount]
+    nnz: int = 0                 # cached Jacobian coefficients per run (0: J v stays matrix-free)
+    n_classes_fj: int = 0
+
+
+# Largest cached Jacobian (coefficients per run) the generator emits: one
+# warp keeps them in shared memory, 4 bytes each in FP32.
+CACHED_JAC_MAX = 2048
 
 
 def _emit_classes(name: str, classes: List[ExprClass], with_v: bool, tables: List[str]) -> Tuple[str, FlopCount]:
@@ -163,6 +170,76 @@ def _emit_classes(name: str, classes: List[ExprClass], with_v: bool, tables: Lis
     return "\n".join(lines), fc
 
 
+def _index_expr(name: str, ci: int, q: int, values: List[int], tables: List[str]) -> str:
+    aff = _affine(values)
+    if aff is not None:
+        return f"{aff[0]} * m + {aff[1]}" if aff[0] != 0 else f"{aff[1]}"
+    tname = f"{name}_c{ci}_s{q}"
+    tables.append(f"    static __device__ const unsigned short {tname}[{len(values)}] = "
+                  f"{{{', '.join(str(v) for v in values)}}};")
+    return f"{tname}[m]"
+
+
+def _emit_cached_jacobian(classes: List[ExprClass], tables: List[str]):
+    """``fj_lanes`` (f and the Jacobian's nonzero coefficients at one state,
+    in one pass that shares the subexpressions of both) and ``jmv_cached``
+    (J v from those coefficients) for classes of the joint expression
+    (f_i, (J v)_i).  A class of M members whose (J v) template reads r
+    components of v stores its coefficients at
+    ``jac[base + j * M + m]`` (slot j, member m), so the lanes of a warp
+    read and write consecutive words."""
+    fj = ["    template <class R> static __device__ CBX_NOINLINE void fj_lanes(const R* __restrict__ ys, "
+          "const R* __restrict__ ps, const R* __restrict__ ds, R t, R* __restrict__ out, R* __restrict__ jac, "
+          "int lane)", "    {", "        (void)ys; (void)ps; (void)ds; (void)t; (void)jac;"]
+    jm = ["    template <class R> static __device__ CBX_NOINLINE void jmv_cached(const R* __restrict__ vs, "
+          "const R* __restrict__ jac, R* __restrict__ out, int lane)", "    {", "        (void)jac; (void)vs;"]
+    fl_fj, fl_jm = FlopCount(), FlopCount()
+    base = 0
+    for ci, c in enumerate(classes):
+        f_t, jv_t = c.template.args
+        nm = len(c.members)
+        slot_syms = [_placeholder(k, j) for (k, j) in c.slots]
+        v_syms = [ph for ph in slot_syms if ph.name[1] == "v"]
+        coefs = [sp.diff(jv_t, v) for v in v_syms]
+        if any(v in cf.free_symbols for cf in coefs for v in v_syms):
+            raise ValueError("Jacobian-vector template is not linear in v")
+        sym_map = {TIME: "t"}
+        for sy in slot_syms:
+            sym_map[sy] = f"s_{sy.name[1:]}"
+        printer = _CudaPrinter(sym_map)
+        out_idx = _index_expr("fj", ci, 99, c.members, tables)
+        head = [f"        // class {ci}: {nm} member(s), {len(v_syms)} coefficient(s) each",
+                f"        for (int m = lane; m < {nm}; m += 32) {{", f"            const int o = {out_idx};"]
+        fj += head
+        jm += head
+        for q, (kind, j) in enumerate(c.slots):
+            col = [row[q] for row in c.indices]
+            idx = _index_expr("cj", ci, q, col, tables)
+            src = {"y": "ys", "v": "vs", "p": "ps", "d": "ds"}[kind]
+            if kind == "v":
+                jm.append(f"            const R s_{kind}{j} = {src}[{idx}];")
+            else:
+                fj.append(f"            const R s_{kind}{j} = {src}[{idx}];")
+        reps, reduced = sp.cse([f_t, *coefs], symbols=sp.numbered_symbols("_t"), optimizations="basic")
+        for sy, e in reps:
+            fj.append(f"            const R {sy} = {printer.doprint(e)};")
+            fl_fj = fl_fj + count_ops(e)
+        fj.append(f"            out[o] = {printer.doprint(reduced[0])};")
+        for k, e in enumerate(reduced):
+            fl_fj = fl_fj + count_ops(e)
+        for j, e in enumerate(reduced[1:]):
+            fj.append(f"            jac[{base + j * nm} + m] = {printer.doprint(e)};")
+        terms = [f"jac[{base + j * nm} + m] * {printer.doprint(v)}" for j, v in enumerate(v_syms)]
+        jm.append(f"            out[o] = {' + '.join(terms) if terms else 'R(0)'};")
+        fl_jm = fl_jm + FlopCount(add=max(len(terms) - 1, 0) * nm, mul=len(terms) * nm)
+        fj.append("        }")
+        jm.append("        }")
+        base += nm * len(v_syms)
+    fj.append("    }")
+    jm.append("    }")
+    return "\n".join(fj), "\n".join(jm), base, fl_fj, fl_jm
+
+
 def generate_warp_system(system: SymbolicODE, struct_name: str = "WarpSystem") -> WarpSystemCode:
     """Class-grouped right-hand side and Jacobian-vector product."""
     n = system.num_states
@@ -189,13 +266,29 @@ def generate_warp_system(system: SymbolicODE, struct_name: str = "WarpSystem") -
     tables: List[str] = []
     body_f, fl_f = _emit_classes("dxdt_lanes", cf, False, tables)
     body_j, fl_j = _emit_classes("jmv_lanes", cj, True, tables)
+    flops = {"dxdt": fl_f, "jmv": fl_j}
+    # J cached at each linearisation: its nonzero coefficients evaluated
+    # together with f, then every J v is a short sum over shared memory
+    nnz = sum(1 for i in range(n) for k in range(n) if J[i, k] != 0)
+    cached, n_fj = [], 0
+    if 0 < nnz <= CACHED_JAC_MAX:
+        cfj = group_classes([sp.Tuple(f[i], jv[i]) for i in range(n)], kind_v)
+        body_fj, body_jc, stored, fl_fj, fl_jc = _emit_cached_jacobian(cfj, tables)
+        cached = [body_fj, body_jc]
+        n_fj = len(cfj)
+        nnz = stored
+        flops.update({"fj": fl_fj, "jmv_cached": fl_jc})
+    else:
+        nnz = 0
     src = [*(t.strip() for t in tables),
            f"struct {struct_name} {{",
            f"    static constexpr int N = {n};",
            f"    static constexpr int NP = {system.num_parameters};",
            f"    static constexpr int ND = {system.num_drivers};",
+           f"    static constexpr int NNZ = {nnz};",
            body_f,
            body_j,
+           *cached,
            "};"]
     return WarpSystemCode(source="\n".join(src), n_classes_f=len(cf), n_classes_jv=len(cj),
-                          flops={"dxdt": fl_f, "jmv": fl_j})
+                          flops=flops, nnz=nnz, n_classes_fj=n_fj)

@@ -23,13 +23,16 @@ def _build(nc, tmp_path):
            "#define CBX_NOINLINE __attribute__((noinline))\nusing std::exp; using std::pow;\n"
            + g.source + "\n" + w.source + r'''
 extern "C" void eval(const double* y, const double* v, const double* p, const double* d, double t, double* f1,
-                     double* f2, double* j1, double* j2) {
+                     double* f2, double* j1, double* j2, double* f3, double* j3) {
     System::dxdt<double>(y, p, d, t, f1);
     double J[System::NJ]; System::jac<double>(y, p, d, t, J); System::jmv<double>(J, v, j1);
+    static double jac[WarpSystem::NNZ > 0 ? WarpSystem::NNZ : 1];
     for (int lane = 0; lane < 32; ++lane) {
         WarpSystem::dxdt_lanes<double>(y, p, d, t, f2, lane);
         WarpSystem::jmv_lanes<double>(y, v, p, d, t, j2, lane);
+        WarpSystem::fj_lanes<double>(y, p, d, t, f3, jac, lane);
     }
+    for (int lane = 0; lane < 32; ++lane) WarpSystem::jmv_cached<double>(v, jac, j3, lane);
 }
 ''')
     cpp = tmp_path / "wg.cpp"
@@ -50,12 +53,17 @@ def test_classes_equal_straight_line_code(nc, tmp_path):
     v = rng.normal(size=N)
     p = np.array([120.0, 36.0, 0.5])
     d = np.array([3.0])
-    f1, f2, j1, j2 = (np.zeros(N) for _ in range(4))
+    f1, f2, j1, j2, f3, j3 = (np.zeros(N) for _ in range(6))
     ptr = lambda a: a.ctypes.data_as(ctypes.c_void_p)
-    L.eval.argtypes = [ctypes.c_void_p] * 4 + [ctypes.c_double] + [ctypes.c_void_p] * 4
-    L.eval(ptr(y), ptr(v), ptr(p), ptr(d), 0.0, ptr(f1), ptr(f2), ptr(j1), ptr(j2))
+    L.eval.argtypes = [ctypes.c_void_p] * 4 + [ctypes.c_double] + [ctypes.c_void_p] * 6
+    L.eval(ptr(y), ptr(v), ptr(p), ptr(d), 0.0, ptr(f1), ptr(f2), ptr(j1), ptr(j2), ptr(f3), ptr(j3))
     np.testing.assert_allclose(f2, f1, rtol=1e-13, atol=1e-12)
     np.testing.assert_allclose(j2, j1, rtol=1e-12, atol=1e-10)
+    # the cached Jacobian: f and J's nonzeros in one class pass, then J v
+    # from the stored coefficients
+    assert w.nnz == 12 * nc - 2 and w.n_classes_fj == 6
+    np.testing.assert_allclose(f3, f1, rtol=1e-13, atol=1e-12)
+    np.testing.assert_allclose(j3, j1, rtol=1e-12, atol=1e-10)
 
 
 def test_non_affine_members_use_index_tables():
