@@ -14,6 +14,7 @@ bit-level comparison with the reference is the generated device code's
 """
 
 import json
+import os
 from pathlib import Path
 
 import numpy as np
@@ -24,8 +25,14 @@ from parity_utils import run_oracle, tol_units
 
 GOLDEN = Path(__file__).resolve().parent / "golden"
 
-F64_CASES = [n for n, c in CASES.items() if c["precision"] == "float64"]
-F32_CASES = [n for n, c in CASES.items() if c["precision"] == "float32"]
+def _param(name):
+    slow = CASES[name].get("slow_oracle") and not os.environ.get("CBX_SLOW_PINS")
+    return pytest.param(name, marks=pytest.mark.skip(reason="minutes of oracle Krylov iterations; "
+                                                             "CBX_SLOW_PINS=1 runs it")) if slow else name
+
+
+F64_CASES = [_param(n) for n, c in CASES.items() if c["precision"] == "float64"]
+F32_CASES = [_param(n) for n, c in CASES.items() if c["precision"] == "float32"]
 
 
 def _load(name):
