@@ -745,7 +745,12 @@ __device__ __forceinline__ bool warp_iterate(WarpLane<Cfg>& L, WarpCtx<Cfg>& w, 
 template <class Cfg>
 __device__ __forceinline__ void run_warp(const cbx_solve_args& a) {
     using R = typename Cfg::R;
-    __shared__ WarpMem<Cfg> mem[Cfg::BLOCK / 32];
+    // the warps' WarpMem records live in dynamic shared memory (their size,
+    // BLOCK / 32 records, is published as the size of cbx_warp_smem_probe
+    // and passed by the launch), so large records are not held to the
+    // 48 KB limit of static shared memory
+    extern __shared__ __align__(16) unsigned char cbx_dyn_smem[];
+    WarpMem<Cfg>* mem = reinterpret_cast<WarpMem<Cfg>*>(cbx_dyn_smem);
     __shared__ BlockTotals bt;
     totals_begin(&bt);
     const int lane = threadIdx.x & 31;
@@ -775,6 +780,7 @@ __device__ __forceinline__ void run_warp(const cbx_solve_args& a) {
 }  // namespace cbx
 
 #define CBX_DEFINE_WARP_KERNEL(CFG)                                                                  \
+    extern "C" __device__ char cbx_warp_smem_probe[sizeof(cbx::WarpMem<CFG>) * (CFG::BLOCK / 32)];      \
     extern "C" __global__ void __launch_bounds__(CFG::BLOCK) cbx_integrate_warp(cbx_solve_args a) {    \
         cbx::run_warp<CFG>(a);                                                                         \
     }

@@ -36,6 +36,7 @@ struct cbx_module {
     bool adj_resolved;
     int n_families;  // families of the heterogeneous kernel (0 without one)
     int primary;     // 1: context is the device's primary context, 0: it is not, -1: not yet checked
+    size_t warp_smem;  // dynamic shared memory of the warp kernel's launch (bytes)
 };
 
 namespace {
@@ -60,6 +61,7 @@ struct DriverApi {
     CBX_DRV(cuModuleUnload)
     CBX_DRV(cuDeviceGetAttribute)
     CBX_DRV(cuFuncGetAttribute)
+    CBX_DRV(cuFuncSetAttribute)
     CBX_DRV(cuOccupancyMaxActiveBlocksPerMultiprocessor)
     CBX_DRV(cuLaunchKernel)
     CBX_DRV(cuGetErrorName)
@@ -96,6 +98,7 @@ bool load_driver() {
     CBX_SYM(cuModuleUnload)
     CBX_SYM(cuDeviceGetAttribute)
     CBX_SYM(cuFuncGetAttribute)
+    CBX_SYM(cuFuncSetAttribute)
     CBX_SYM(cuOccupancyMaxActiveBlocksPerMultiprocessor)
     CBX_SYM(cuLaunchKernel)
     CBX_SYM(cuGetErrorName)
@@ -259,6 +262,25 @@ int cbx_module_load(const void* cubin, size_t cubin_size, int device, cbx_module
         delete m;
         return fail(CBX_ERR_ARGUMENT, "the cubin defines none of the integration kernels");
     }
+    if (m->fn[CBX_KERNEL_WARP]) {
+        // the warp kernel's per-warp records: dynamic shared memory sized by
+        // its probe symbol, opted in above the default 48 KB
+        CUdeviceptr probe = 0;
+        size_t bytes = 0;
+        if (g_drv.cuModuleGetGlobal(&probe, &bytes, m->module, "cbx_warp_smem_probe") == CUDA_SUCCESS) {
+            m->warp_smem = bytes;
+            if (bytes > 48 * 1024) {
+                int rc2 = check_cu(g_drv.cuFuncSetAttribute(m->fn[CBX_KERNEL_WARP],
+                                                            CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES,
+                                                            (int)bytes), "cuFuncSetAttribute");
+                if (rc2) {
+                    g_drv.cuModuleUnload(m->module);
+                    delete m;
+                    return rc2;
+                }
+            }
+        }
+    }
     if (m->fn[CBX_KERNEL_HETERO]) {
         CUdeviceptr probe = 0;
         size_t fams = 0;
@@ -309,7 +331,9 @@ int cbx_kernel_info(cbx_module* module, int kernel, int* registers, int* local_b
 int cbx_occupancy(cbx_module* module, int kernel, int block, int* blocks_per_sm) {
     if (!module || kernel < 0 || kernel > 3 || !module->fn[kernel] || block <= 0 || !blocks_per_sm)
         return fail(CBX_ERR_ARGUMENT, "bad occupancy query");
-    return check_cu(g_drv.cuOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, module->fn[kernel], block, 0),
+    const size_t smem = kernel == CBX_KERNEL_WARP ? module->warp_smem : 0;
+    return check_cu(g_drv.cuOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, module->fn[kernel], block,
+                                                                      smem),
                     "cuOccupancyMaxActiveBlocksPerMultiprocessor");
 }
 
@@ -353,8 +377,9 @@ int cbx_solve(cbx_module* module, const cbx_solve_args* args, int kernel, int bl
             g = (args->n_runs + block - 1) / block;
         } else {
             int per_sm = 0;
-            if (g_drv.cuOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, module->fn[kernel], block, 0) != CUDA_SUCCESS ||
-                per_sm <= 0)
+            const size_t smem = kernel == CBX_KERNEL_WARP ? module->warp_smem : 0;
+            if (g_drv.cuOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, module->fn[kernel], block, smem) !=
+                    CUDA_SUCCESS || per_sm <= 0)
                 per_sm = 1;
             g = (long long)per_sm * module->sm_count;
             const long long runs_per_block = kernel == CBX_KERNEL_WARP ? block / 32 : block;
@@ -363,9 +388,12 @@ int cbx_solve(cbx_module* module, const cbx_solve_args* args, int kernel, int bl
         }
     }
     if (g > 2147483647LL) return fail(CBX_ERR_ARGUMENT, "grid too large");
+    if (kernel == CBX_KERNEL_WARP && module->warp_smem == 0)
+        return fail(CBX_ERR_ARGUMENT, "the warp kernel's module publishes no shared-memory size");
+    const unsigned smem = kernel == CBX_KERNEL_WARP ? (unsigned)module->warp_smem : 0u;
     cbx_solve_args local = *args;
     void* params[] = {&local};
-    return check_cu(g_drv.cuLaunchKernel(module->fn[kernel], (unsigned)g, 1, 1, (unsigned)block, 1, 1, 0,
+    return check_cu(g_drv.cuLaunchKernel(module->fn[kernel], (unsigned)g, 1, 1, (unsigned)block, 1, 1, smem,
                                    static_cast<CUstream>(stream), params, nullptr),
                     "cuLaunchKernel");
 }
