@@ -540,7 +540,14 @@ def cable_arm(args, dev, peak_fp32=None):
         from cubie_b200.perfmodel import estimate_flops
         spec = s32.kernel_spec(s32._timing(T), ArrayInterpolator.from_system(sys32, drv, np.float32).device_meta())
         wc = s32._system_code["warp"]
-        fl = estimate_flops(spec, SimpleNamespace(n=sys32.num_states, flops=wc.flops), r.totals)
+        wf = {k: v.flops for k, v in wc.flops.items()}
+        if wc.nnz > 0:
+            # cached Jacobian: f and J's coefficients in one pass per Newton
+            # iteration, every J v a sum over the stored coefficients
+            wf = {"dxdt": wf["dxdt"], "jac": wf["fj"] - wf["dxdt"], "jmv": wf["jmv_cached"]}
+        fl = estimate_flops(spec, SimpleNamespace(n=sys32.num_states,
+                                                  flops={k: SimpleNamespace(flops=v) for k, v in wf.items()}),
+                            r.totals)
         roof = {"bound": "fp32", "achieved": fl / (ms * 1e-3) / 1e12, "peak": peak_fp32, "unit": "TFLOP/s",
                 "frac": fl / (ms * 1e-3) / 1e12 / peak_fp32, "flops_per_launch": fl,
                 "flop_source": "generated f and J v DAGs x the launch's step, Newton and Krylov totals"}

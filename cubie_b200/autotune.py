@@ -1,16 +1,23 @@
 """Launch-shape autotuner for the integration kernels.
 
 For one solver configuration it compiles the kernel at a set of launch
-shapes (block size, and a minimum of resident blocks per SM, which caps
-registers per thread), times the persistent launch of each on a sample of
-the caller's batch with CUDA events, and keeps the fastest.  Results are
+shapes (block size, i.e. warps per block, and a minimum of resident blocks
+per SM, which caps registers per thread) and, for the warp-per-system
+layout, scratch placements (the stage solve's scratch vectors in the warp's
+shared memory or in the lanes' registers and local memory; the reference
+makes the same shared-versus-local choice per buffer with a fixed table,
+src/cubie/integrators/memory_heuristics.py:99-116), times the persistent
+launch of each on a sample of the caller's batch with CUDA events, and
+keeps the fastest.  Results are
 cached on disk per configuration and GPU (``CUBIE_B200_CACHE_DIR``, default
 ``~/.cache/cubie_b200``, file ``autotune.json``), so a configuration is
 tuned once per machine.  The reference picks its block size by a
 shared-memory limit only (``limit_blocksize``,
 src/cubie/batchsolving/BatchSolverKernel.py:780-830).
 
-``Solver(..., block_size="auto")`` runs it on the first solve.
+``Solver(..., block_size="auto")`` (shapes) and
+``Solver(..., layout="warp", scratch_placement="auto")`` (shapes and
+placements) run it on the first solve.
 """
 
 from __future__ import annotations
@@ -28,6 +35,24 @@ DEFAULT_CANDIDATES: Tuple[Tuple[int, int], ...] = ((128, 1), (64, 1), (256, 1), 
                                                     (64, 8), (256, 2))
 
 
+# warp-per-system layout: fewer shapes (each compile of a large system is
+# costly), each with both scratch placements
+WARP_CANDIDATES: Tuple[Tuple[int, int, str], ...] = tuple(
+    (b, 1, p) for b in (128, 64, 256) for p in ("shared", "local"))
+
+
+# runs of the caller's batch timed per candidate
+SAMPLE_RUNS = 8192
+
+
+def default_candidates(solver) -> List[Tuple]:
+    if solver.layout == "warp":
+        if getattr(solver, "placement_pending", False):
+            return list(WARP_CANDIDATES)
+        return [(b, 1, solver.scratch_placement) for b in (128, 64, 256)]
+    return list(DEFAULT_CANDIDATES)
+
+
 def _cache_path() -> Path:
     d = os.environ.get("CUBIE_B200_CACHE_DIR")
     p = Path(d) if d else Path.home() / ".cache" / "cubie_b200"
@@ -39,12 +64,13 @@ def config_key(solver, duration: float, gpu_name: str) -> str:
     """Configuration identity without the launch shape."""
     variant = copy.copy(solver)
     variant.block_size, variant.min_blocks_per_sm = 128, 1
+    variant.scratch_placement = "shared"
     variant.__dict__["_prepared"] = {}
     src = variant.prepare(duration, load=False)["gen"].source
     return hashlib.sha256((src + gpu_name).encode()).hexdigest()[:24]
 
 
-def choose(timings: Dict[Tuple[int, int], float]) -> Tuple[int, int]:
+def choose(timings: Dict[Tuple, float]) -> Tuple:
     """Fastest shape; ties go to the earlier candidate (stable order)."""
     best = None
     for shape, ms in timings.items():
@@ -57,22 +83,28 @@ def choose(timings: Dict[Tuple[int, int], float]) -> Tuple[int, int]:
     return best
 
 
-def variant(solver, block: int, min_blocks: int):
+def variant(solver, block: int, min_blocks: int, placement: Optional[str] = None):
     v = copy.copy(solver)
     v.block_size = int(block)
     v.min_blocks_per_sm = int(min_blocks)
+    if placement is not None:
+        v.scratch_placement = placement
     v.__dict__["_prepared"] = {}
     return v
 
 
+def _label(shape: Tuple) -> str:
+    return "x".join(str(x) for x in shape)
+
+
 def autotune(solver, inits, params, duration: float, durations=None, candidates: Optional[Sequence] = None,
-             repeats: int = 2, timer: Optional[Callable] = None, use_cache: bool = True) -> Dict:
+             repeats: int = 2, timer: Optional[Callable] = None, use_cache: bool = True, interp=None) -> Dict:
     """Time the persistent launch at each candidate shape on the given
     batch (device tensors or arrays ``[n_states, n]``, ``[n_params, n]``)
     and return ``{"block", "min_blocks", "timings_ms", "cached"}``.
 
     ``timer(variant_solver) -> ms`` replaces the GPU measurement (tests)."""
-    cands = [tuple(c) for c in (candidates or DEFAULT_CANDIDATES)]
+    cands = [tuple(c) for c in (candidates or default_candidates(solver))]
     gpu = "cpu-test" if timer is not None else _gpu_name(solver.device)
     key = config_key(solver, duration, gpu)
     store = {}
@@ -82,18 +114,21 @@ def autotune(solver, inits, params, duration: float, durations=None, candidates:
             store = json.loads(path.read_text())
         except ValueError:
             store = {}
+    key = key + "".join(f"|{_label(c)}" for c in cands)
     if use_cache and key in store:
         hit = store[key]
-        return dict(block=hit["block"], min_blocks=hit["min_blocks"], timings_ms=hit["timings_ms"], cached=True)
-    measure = timer or _gpu_timer(inits, params, duration, durations, repeats)
+        return dict(block=hit["block"], min_blocks=hit["min_blocks"], placement=hit.get("placement"),
+                    timings_ms=hit["timings_ms"], cached=True)
+    measure = timer or _gpu_timer(inits, params, duration, durations, repeats, interp)
     timings = {}
-    for block, minb in cands:
+    for shape in cands:
         try:
-            timings[(block, minb)] = float(measure(variant(solver, block, minb)))
+            timings[shape] = float(measure(variant(solver, *shape)))
         except Exception:  # a shape that cannot compile or launch is skipped
-            timings[(block, minb)] = float("nan")
-    block, minb = choose(timings)
-    result = dict(block=block, min_blocks=minb, timings_ms={f"{b}x{m}": t for (b, m), t in timings.items()})
+            timings[shape] = float("nan")
+    best = choose(timings)
+    result = dict(block=best[0], min_blocks=best[1], placement=best[2] if len(best) > 2 else None,
+                  timings_ms={_label(c): t for c, t in timings.items()})
     if use_cache:
         store[key] = result
         tmp = path.with_suffix(f".tmp{os.getpid()}")
@@ -107,25 +142,35 @@ def _gpu_name(device: int) -> str:
     return torch.cuda.get_device_name(device)
 
 
-def _gpu_timer(inits, params, duration, durations, repeats):
+def _gpu_timer(inits, params, duration, durations, repeats, interp=None):
+    """Best of ``repeats`` persistent launches of a variant on the caller's
+    batch (driven systems with the caller's driver table)."""
     torch = __import__("torch")
 
     def measure(v) -> float:
         dev = torch.device("cuda", v.device)
         tdt = torch.float32 if v.precision == np.float32 else torch.float64
-        it = torch.as_tensor(inits, device=dev).to(tdt).contiguous()
-        pt = torch.as_tensor(params, device=dev).to(tdt).contiguous()
-        dt = torch.as_tensor(durations, device=dev, dtype=torch.float64) if durations is not None else None
+        # a sample of the batch (a few resident waves) is timed
+        k = min(int(inits.shape[1]), SAMPLE_RUNS)
+        it = torch.as_tensor(inits[:, :k], device=dev).to(tdt).contiguous()
+        pt = torch.as_tensor(params[:, :k], device=dev).to(tdt).contiguous()
+        dt = torch.as_tensor(np.asarray(durations)[:k] if not hasattr(durations, "device") else durations[:k],
+                             device=dev, dtype=torch.float64) if durations is not None else None
         n = int(it.shape[1])
-        prep = v.prepare(duration, durations=durations)
+        prep = v.prepare(duration, interp=interp, durations=durations)
+        coeff = None
+        if interp is not None:
+            coeff = torch.as_tensor(interp.coefficients.astype(v.precision), device=dev).contiguous()
+        elif v.system.num_drivers > 0:
+            raise ValueError("a driven system is tuned with its driver table")
         bufs = v.allocate_outputs(prep, n, dev, tdt)
         stream = torch.cuda.current_stream(dev)
         best = float("inf")
         for _ in range(max(1, repeats)):
-            a = v.make_args(prep, bufs, it, pt, None, n, duration, 0.0, 0.0, dt)
+            a = v.make_args(prep, bufs, it, pt, coeff, n, duration, 0.0, 0.0, dt)
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            prep["module"].launch(a, 1, v.block_size, 0, stream.cuda_stream)
+            prep["module"].launch(a, v.launch_kind, v.block_size, 0, stream.cuda_stream)
             e1.record(stream)
             e1.synchronize()
             best = min(best, e0.elapsed_time(e1))

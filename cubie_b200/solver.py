@@ -565,12 +565,18 @@ class Solver:
         torch = _torch()
         if not torch.cuda.is_available():
             raise RuntimeError("cubie_b200 needs a CUDA device: no GPU is visible")
-        if self.autotune_pending:
-            from .autotune import autotune
-            tuned = autotune(self, inits, params, duration, durations=durations)
+        if self.autotune_pending or self.placement_pending:
+            from .autotune import autotune, default_candidates
+            cands = default_candidates(self)
+            if not self.autotune_pending:
+                # placement only: keep the caller's launch shape
+                cands = [c for c in cands if c[0] == self.block_size] or cands
+            tuned = autotune(self, inits, params, duration, durations=durations, candidates=cands, interp=interp)
             self.block_size, self.min_blocks_per_sm = int(tuned["block"]), int(tuned["min_blocks"])
+            if tuned.get("placement"):
+                self.scratch_placement = tuned["placement"]
             self.autotune_result = tuned
-            self.autotune_pending = False
+            self.autotune_pending = self.placement_pending = False
             self.__dict__["_prepared"] = {}
         prep = self.prepare(duration, settling_time, t0, interp, durations)
         spec: KernelSpec = prep["spec"]

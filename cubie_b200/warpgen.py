@@ -93,6 +93,11 @@ def group_classes(exprs: Sequence[sp.Expr], kind_of: Dict[sp.Symbol, Tuple[str, 
     return [classes[k] for k in order]
 
 
+def _times(fc: FlopCount, k: int) -> FlopCount:
+    """The operation count of ``k`` evaluations of one class body."""
+    return FlopCount(fc.add * k, fc.mul * k, fc.div * k, fc.special * k)
+
+
 def _affine(values: List[int]):
     """(a, b) with values[m] == a * m + b for every m, or None."""
     if len(values) == 1:
@@ -162,9 +167,9 @@ def _emit_classes(name: str, classes: List[ExprClass], with_v: bool, tables: Lis
         reps, reduced = sp.cse([c.template], symbols=sp.numbered_symbols("_t"), optimizations="basic")
         for s, e in reps:
             lines.append(f"            const R {s} = {printer.doprint(e)};")
-            fc = fc + count_ops(e)
+            fc = fc + _times(count_ops(e), nm)
         lines.append(f"            out[o] = {printer.doprint(reduced[0])};")
-        fc = fc + count_ops(reduced[0])
+        fc = fc + _times(count_ops(reduced[0]), nm)
         lines.append("        }")
     lines.append("    }")
     return "\n".join(lines), fc
@@ -223,10 +228,10 @@ def _emit_cached_jacobian(classes: List[ExprClass], tables: List[str]):
         reps, reduced = sp.cse([f_t, *coefs], symbols=sp.numbered_symbols("_t"), optimizations="basic")
         for sy, e in reps:
             fj.append(f"            const R {sy} = {printer.doprint(e)};")
-            fl_fj = fl_fj + count_ops(e)
+            fl_fj = fl_fj + _times(count_ops(e), nm)
         fj.append(f"            out[o] = {printer.doprint(reduced[0])};")
         for k, e in enumerate(reduced):
-            fl_fj = fl_fj + count_ops(e)
+            fl_fj = fl_fj + _times(count_ops(e), nm)
         for j, e in enumerate(reduced[1:]):
             fj.append(f"            jac[{base + j * nm} + m] = {printer.doprint(e)};")
         terms = [f"jac[{base + j * nm} + m] * {printer.doprint(v)}" for j, v in enumerate(v_syms)]

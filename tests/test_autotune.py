@@ -54,3 +54,32 @@ def test_config_key_ignores_launch_shape():
 def test_block_size_auto_is_pending_until_first_solve():
     s = _solver(block_size="auto")
     assert s.autotune_pending and s.block_size == 128
+
+
+def test_warp_layout_tunes_scratch_placement(tmp_path, monkeypatch):
+    """With scratch_placement='auto' the warp layout's candidates carry both
+    placements; the fastest shape and placement win and are cached."""
+    from cubie_b200 import Solver, create_ODE_system
+    from cubie_b200.autotune import autotune, default_candidates
+    monkeypatch.setenv("CUBIE_B200_CACHE_DIR", str(tmp_path))
+    sysm = create_ODE_system(VDP, states={"x": 2.0, "y": 0.0}, parameters={"mu": 10.0}, precision=np.float32)
+    s = Solver(sysm, algorithm="l_stable_dirk_3", layout="warp", scratch_placement="auto",
+               output_types=["state"])
+    assert s.placement_pending and s.scratch_placement == "shared"
+    cands = default_candidates(s)
+    assert {c[2] for c in cands} == {"shared", "local"} and all(len(c) == 3 for c in cands)
+    seen = []
+
+    def fake(v):
+        seen.append((v.block_size, v.scratch_placement))
+        return 5.0 if (v.block_size, v.scratch_placement) == (64, "local") else 9.0
+
+    r = autotune(s, None, None, 2.0, candidates=cands, timer=fake)
+    assert (r["block"], r["placement"], r["cached"]) == (64, "local", False)
+    assert sorted(seen) == sorted((c[0], c[2]) for c in cands)
+    assert autotune(s, None, None, 2.0, candidates=cands, timer=fake)["cached"]
+    # the placement is part of the generated source, not of the cache key
+    fixed = Solver(sysm, algorithm="l_stable_dirk_3", layout="warp", scratch_placement="local",
+                   output_types=["state"])
+    assert "SHARED_SCRATCH = false" in fixed.prepare(2.0, load=False)["gen"].source
+    assert "SHARED_SCRATCH = true" in s.prepare(2.0, load=False)["gen"].source
