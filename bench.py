@@ -510,7 +510,7 @@ def cable_arm(args, dev, peak_fp32=None):
     t_s = np.arange(1000) * 0.01
     drv = {"driver_sample_period": 0.01, "t0": 0.0, "order": 3, "wrap": False, "I": np.where(t_s < 5.0, 10.0, 0.0)}
     kw = dict(algorithm="l_stable_dirk_3", linear_correction_type="bicgstab", layout="warp", dt=0.025,
-              scratch_placement=args.c3_placement,
+              scratch_placement=args.c3_placement, max_registers=args.c3_max_registers,
               output_types=["mean", "max", "peaks[3]"], summarise_every=T, sample_summaries_every=0.1,
               summarise_variables=[f"V{j:02d}" for j in range(nc)], device=dev.index, max_steps=100000)
     sys32 = create_ODE_system(eqs, states=states, parameters=params, drivers=drivers, precision=np.float32)
@@ -890,6 +890,8 @@ def main():
     ap.add_argument("--c3-steps", type=int, default=2)
     ap.add_argument("--c3-placement", default="shared", choices=["shared", "local", "auto"],
                     help="stage-solve scratch placement of the cable's warp kernel")
+    ap.add_argument("--c3-max-registers", type=int, default=0, help="register cap of the cable's warp kernel "
+                    "(0: the compiler's default)")
     ap.add_argument("--adj-steps", type=int, default=3)
     ap.add_argument("--adj-warmup", type=int, default=3)
     ap.add_argument("--leg", default=None, choices=["adjoint", "lorenz", "cable", "hetero"],

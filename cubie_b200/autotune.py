@@ -37,8 +37,8 @@ DEFAULT_CANDIDATES: Tuple[Tuple[int, int], ...] = ((128, 1), (64, 1), (256, 1), 
 
 # warp-per-system layout: fewer shapes (each compile of a large system is
 # costly), each with both scratch placements
-WARP_CANDIDATES: Tuple[Tuple[int, int, str], ...] = tuple(
-    (b, 1, p) for b in (128, 64, 256) for p in ("shared", "local"))
+WARP_CANDIDATES: Tuple[Tuple[int, int, str, int], ...] = tuple(
+    (b, 1, p, r) for b in (128, 64) for p in ("shared", "local") for r in (0, 168))
 
 
 # runs of the caller's batch timed per candidate
@@ -49,7 +49,7 @@ def default_candidates(solver) -> List[Tuple]:
     if solver.layout == "warp":
         if getattr(solver, "placement_pending", False):
             return list(WARP_CANDIDATES)
-        return [(b, 1, solver.scratch_placement) for b in (128, 64, 256)]
+        return [(b, 1, solver.scratch_placement, r) for b in (128, 64) for r in (0, 168)]
     return list(DEFAULT_CANDIDATES)
 
 
@@ -65,6 +65,7 @@ def config_key(solver, duration: float, gpu_name: str) -> str:
     variant = copy.copy(solver)
     variant.block_size, variant.min_blocks_per_sm = 128, 1
     variant.scratch_placement = "shared"
+    variant.max_registers = 0
     variant.__dict__["_prepared"] = {}
     src = variant.prepare(duration, load=False)["gen"].source
     return hashlib.sha256((src + gpu_name).encode()).hexdigest()[:24]
@@ -83,12 +84,15 @@ def choose(timings: Dict[Tuple, float]) -> Tuple:
     return best
 
 
-def variant(solver, block: int, min_blocks: int, placement: Optional[str] = None):
+def variant(solver, block: int, min_blocks: int, placement: Optional[str] = None,
+            max_registers: Optional[int] = None):
     v = copy.copy(solver)
     v.block_size = int(block)
     v.min_blocks_per_sm = int(min_blocks)
     if placement is not None:
         v.scratch_placement = placement
+    if max_registers is not None:
+        v.max_registers = int(max_registers)
     v.__dict__["_prepared"] = {}
     return v
 
@@ -118,7 +122,7 @@ def autotune(solver, inits, params, duration: float, durations=None, candidates:
     if use_cache and key in store:
         hit = store[key]
         return dict(block=hit["block"], min_blocks=hit["min_blocks"], placement=hit.get("placement"),
-                    timings_ms=hit["timings_ms"], cached=True)
+                    max_registers=hit.get("max_registers"), timings_ms=hit["timings_ms"], cached=True)
     measure = timer or _gpu_timer(inits, params, duration, durations, repeats, interp)
     timings = {}
     for shape in cands:
@@ -128,6 +132,7 @@ def autotune(solver, inits, params, duration: float, durations=None, candidates:
             timings[shape] = float("nan")
     best = choose(timings)
     result = dict(block=best[0], min_blocks=best[1], placement=best[2] if len(best) > 2 else None,
+                  max_registers=best[3] if len(best) > 3 else None,
                   timings_ms={_label(c): t for c, t in timings.items()})
     if use_cache:
         store[key] = result

@@ -56,6 +56,7 @@ struct WarpMem {
     R sbase[SH];                          // stage base state (shared placement)
     R sstart[SH];                         // step start state (shared placement)
     R r0[Cfg::SHARED_SCRATCH ? 32 * ((N + 31) / 32) : 1];  // BiCGSTAB shadow residual (shared placement)
+    R sz[Cfg::SHARED_SCRATCH ? 32 * ((N + 31) / 32) : 1];  // stage increment in and out of the solve
     R p[Cfg::NP > 0 ? Cfg::NP : 1];
     R d[Cfg::ND > 0 ? Cfg::ND : 1];       // drivers of the evaluation
     R dlin[Cfg::ND > 0 ? Cfg::ND : 1];    // drivers at the linearisation point
@@ -71,7 +72,7 @@ struct WarpCtx {
     int lane;
     const R* coeffs;
     C tol_scale;
-    R tlin;
+    mutable R tlin;
 
     __device__ __forceinline__ bool valid(int k) const { return lane + 32 * k < N; }
     __device__ __forceinline__ void put(R* dst, const R* loc) const {
@@ -89,7 +90,7 @@ struct WarpCtx {
             if (lane == q) dst[q] = drv[q];
     }
     // f(t, y): y and f local.
-    __device__ __forceinline__ void rhs(const R* yloc, R t, const R* drv, R* floc) {
+    __device__ __forceinline__ void rhs(const R* yloc, R t, const R* drv, R* floc) const {
         put(m->ys, yloc);
         put_drivers(m->d, drv);
         __syncwarp();
@@ -98,7 +99,7 @@ struct WarpCtx {
         get(m->out, floc);
         __syncwarp();
     }
-    __device__ __forceinline__ void linearize(const R* Yloc, R t, const R* drv) {
+    __device__ __forceinline__ void linearize(const R* Yloc, R t, const R* drv) const {
         if constexpr (CACHED) {
             R scratch[L];
             rhs_linearize(Yloc, t, drv, scratch);
@@ -112,7 +113,7 @@ struct WarpCtx {
     // f(t, Y) and the linearisation at Y in one pass: with a cached
     // Jacobian, f and J's coefficients share their subexpressions (the
     // exponentials of a gating rate appear in both).
-    __device__ __forceinline__ void rhs_linearize(const R* Yloc, R t, const R* drv, R* floc) {
+    __device__ __forceinline__ void rhs_linearize(const R* Yloc, R t, const R* drv, R* floc) const {
         if constexpr (CACHED) {
             put(m->ys, Yloc);
             put_drivers(m->d, drv);
@@ -127,7 +128,7 @@ struct WarpCtx {
         }
     }
     // J(y_lin) v: v and the result local.
-    __device__ __forceinline__ void jmv(const R* vloc, R* outloc) {
+    __device__ __forceinline__ void jmv(const R* vloc, R* outloc) const {
         put(m->vs, vloc);
         __syncwarp();
         if constexpr (CACHED) {
@@ -152,11 +153,11 @@ struct WarpStageOp {
     static constexpr int K = WarpCtx<Cfg>::L;
     static constexpr int KT = Cfg::N;
     static constexpr bool SHADOW_SHARED = Cfg::SHARED_SCRATCH;
-    WarpCtx<Cfg>* w;
+    WarpCtx<Cfg> w;   // by value: no address of the solve's state is taken
     R s;
     __device__ __forceinline__ void apply(const R* v, R* out) const {
         R jv[K];
-        w->jmv(v, jv);
+        w.jmv(v, jv);
 #pragma unroll
         for (int i = 0; i < K; ++i) out[i] = v[i] - s * jv[i];
     }
@@ -165,29 +166,29 @@ struct WarpStageOp {
         for (int i = 0; i < K; ++i) out[i] = v[i];
 #pragma unroll 1
         for (int k = 0; k < Cfg::PRECOND_ORDER; ++k) {
-            w->jmv(out, scratch);
+            w.jmv(out, scratch);
 #pragma unroll
             for (int i = 0; i < K; ++i) out[i] = v[i] + s * scratch[i];
         }
     }
     __device__ __forceinline__ C tol(int i) const {
-        const int c = w->lane + 32 * i;
-        return c < Cfg::N ? C(R(1) / w->m->kw[c]) : C(1);
+        const int c = w.lane + 32 * i;
+        return c < Cfg::N ? C(R(1) / w.m->kw[c]) : C(1);
     }
     __device__ __forceinline__ C wnorm2(const R* v) const {
         R s2 = R(0);
 #pragma unroll
         for (int i = 0; i < K; ++i) {
-            if (w->valid(i)) {
-                const R ratio = v[i] * w->m->kw[w->lane + 32 * i];
+            if (w.valid(i)) {
+                const R ratio = v[i] * w.m->kw[w.lane + 32 * i];
                 s2 += ratio * ratio;
             }
         }
         return C(warp_sum(s2) * (R(1) / R(Cfg::N)));
     }
     // BiCGSTAB's shadow residual in shared memory (shared placement)
-    __device__ __forceinline__ R* shadow() const { return w->m->r0; }
-    __device__ __forceinline__ int slot(int i) const { return w->lane + 32 * i; }
+    __device__ __forceinline__ R* shadow() const { return w.m->r0; }
+    __device__ __forceinline__ int slot(int i) const { return w.lane + 32 * i; }
     template <class T>
     __device__ __forceinline__ T reduce(T partial) const { return warp_sum(partial); }
 };
@@ -201,33 +202,34 @@ struct WarpDirkProblem {
     using R = typename Cfg::R;
     using C = typename Cfg::C;
     static constexpr int K = WarpCtx<Cfg>::L;
+    static constexpr int ND = Cfg::ND;
     static constexpr bool FUSED = true;
-    WarpCtx<Cfg>* w;
+    WarpCtx<Cfg> w;   // by value: no address of the solve's state is taken
     const R* base;
     const R* step_start;
-    const R* drv;
+    R drv[ND > 0 ? ND : 1];
     R t, h, a;
     __device__ __forceinline__ R b(int k) const {
-        if constexpr (Cfg::SHARED_SCRATCH) return w->valid(k) ? w->m->sbase[w->lane + 32 * k] : R(0);
+        if constexpr (Cfg::SHARED_SCRATCH) return w.valid(k) ? w.m->sbase[w.lane + 32 * k] : R(0);
         else return base[k];
     }
     __device__ __forceinline__ R y0(int k) const {
-        if constexpr (Cfg::SHARED_SCRATCH) return w->valid(k) ? w->m->sstart[w->lane + 32 * k] : R(0);
+        if constexpr (Cfg::SHARED_SCRATCH) return w.valid(k) ? w.m->sstart[w.lane + 32 * k] : R(0);
         else return step_start[k];
     }
     __device__ __forceinline__ void residual(const R* z, R* out) const {
         R Y[K], f[K];
 #pragma unroll
         for (int k = 0; k < K; ++k) Y[k] = b(k) + a * z[k];
-        w->rhs(Y, t, drv, f);
+        w.rhs(Y, t, drv, f);
 #pragma unroll
-        for (int k = 0; k < K; ++k) out[k] = w->valid(k) ? z[k] - h * f[k] : R(0);
+        for (int k = 0; k < K; ++k) out[k] = w.valid(k) ? z[k] - h * f[k] : R(0);
     }
     __device__ __forceinline__ void linearize(const R* z) {
         R Y[K];
 #pragma unroll
         for (int k = 0; k < K; ++k) Y[k] = b(k) + a * z[k];
-        w->linearize(Y, t, drv);
+        w.linearize(Y, t, drv);
     }
     // residual and linearisation at the same iterate (the Newton loop
     // evaluates both at every iteration)
@@ -235,9 +237,9 @@ struct WarpDirkProblem {
         R Y[K], f[K];
 #pragma unroll
         for (int k = 0; k < K; ++k) Y[k] = b(k) + a * z[k];
-        w->rhs_linearize(Y, t, drv, f);
+        w.rhs_linearize(Y, t, drv, f);
 #pragma unroll
-        for (int k = 0; k < K; ++k) out[k] = w->valid(k) ? z[k] - h * f[k] : R(0);
+        for (int k = 0; k < K; ++k) out[k] = w.valid(k) ? z[k] - h * f[k] : R(0);
     }
     __device__ __forceinline__ WarpStageOp<Cfg> op() const { return WarpStageOp<Cfg>{w, a * h}; }
     // Krylov weights 1 / max(katol + krtol * scale * |base|, 1e-16), once per
@@ -245,9 +247,9 @@ struct WarpDirkProblem {
     __device__ __forceinline__ void form_weights() const {
 #pragma unroll
         for (int k = 0; k < K; ++k) {
-            if (!w->valid(k)) continue;
-            const int c = w->lane + 32 * k;
-            w->m->kw[c] = R(C(1) / krylov_tol<Cfg>(c, b(k), w->tol_scale));
+            if (!w.valid(k)) continue;
+            const int c = w.lane + 32 * k;
+            w.m->kw[c] = R(C(1) / krylov_tol<Cfg>(c, b(k), w.tol_scale));
         }
         __syncwarp();
     }
@@ -255,11 +257,11 @@ struct WarpDirkProblem {
         C nrm2 = C(0);
 #pragma unroll
         for (int k = 0; k < K; ++k) {
-            if (!w->valid(k)) continue;
-            const int c = w->lane + 32 * k;
+            if (!w.valid(k)) continue;
+            const int c = w.lane + 32 * k;
             const R sv = b(k) + a * z[k];
             const R ref = pymax(absv(sv), absv(y0(k)));
-            C tol = C(Cfg::natol(c)) + C(Cfg::nrtol(c)) * w->tol_scale * C(ref);
+            C tol = C(Cfg::natol(c)) + C(Cfg::nrtol(c)) * w.tol_scale * C(ref);
             tol = pymax(tol, C(1e-16));
             const C ratio = C(delta[k]) / tol;
             nrm2 += ratio * ratio;
@@ -296,16 +298,33 @@ struct WarpDirkStep {
     // runs 24 % faster.  Moving the operator and norm helpers out of line
     // as well (98 KB) was slower again: their calls pass the per-lane
     // vectors through the stack.
-    static __device__ CBX_NOINLINE int stage_solve(WarpCtx<Cfg>& w, const R* base, const R* y, const R* drv_stage,
-                                                      R stage_time, R dt, R a, Persist& ps, Iters& its) {
-        WarpDirkProblem<Cfg> prob{&w, base, y, drv_stage, stage_time, dt, a};
+    // The context comes by value and the stage increment in a register
+    // array: passing the caller's context or increment by reference kept
+    // them in local memory, reloaded after every shared-memory store.  With
+    // the shared placement the increment crosses the call through shared
+    // memory; otherwise through ``z_io``.
+    static __device__ CBX_NOINLINE int stage_solve(WarpCtx<Cfg> w, const R* base, const R* y, const R* drv_stage,
+                                                      R stage_time, R dt, R a, R* z_io, C& theta, int2& iters) {
+        WarpDirkProblem<Cfg> prob{w, base, y, {}, stage_time, dt, a};
+#pragma unroll
+        for (int q = 0; q < ND; ++q) prob.drv[q] = drv_stage[q];
         prob.form_weights();
+        R u[L];
+#pragma unroll
+        for (int k = 0; k < L; ++k) {
+            if constexpr (Cfg::SHARED_SCRATCH) u[k] = w.m->sz[w.lane + 32 * k];
+            else u[k] = z_io[k];
+        }
+        C th = theta;
         int ni = 0, ki = 0;
-        const int st = newton_solve<Cfg>(prob, ps.z, ps.theta, ni, ki);
-        its.nit = ni;
-        its.kit = ki;
-        its.nit_all += ni;
-        its.kit_all += ki;
+        const int st = newton_solve<Cfg>(prob, u, th, ni, ki);
+        theta = th;
+#pragma unroll
+        for (int k = 0; k < L; ++k) {
+            if constexpr (Cfg::SHARED_SCRATCH) w.m->sz[w.lane + 32 * k] = u[k];
+            else z_io[k] = u[k];
+        }
+        iters = make_int2(ni, ki);
         return st;
     }
     // With the shared placement the stage base goes to shared memory before
@@ -314,12 +333,21 @@ struct WarpDirkStep {
     static __device__ __forceinline__ int solve_stage(WarpCtx<Cfg>& w, const R* base, const R* y,
                                                       const R* drv_stage, R stage_time, R dt, R a, Persist& ps,
                                                       Iters& its) {
+        int2 it2;
+        int st;
         if constexpr (Cfg::SHARED_SCRATCH) {
             w.put(w.m->sbase, base);
-            return stage_solve(w, nullptr, nullptr, drv_stage, stage_time, dt, a, ps, its);
+            w.put(w.m->sz, ps.z);
+            st = stage_solve(w, nullptr, nullptr, drv_stage, stage_time, dt, a, nullptr, ps.theta, it2);
+            w.get(w.m->sz, ps.z);
         } else {
-            return stage_solve(w, base, y, drv_stage, stage_time, dt, a, ps, its);
+            st = stage_solve(w, base, y, drv_stage, stage_time, dt, a, ps.z, ps.theta, it2);
         }
+        its.nit = it2.x;
+        its.kit = it2.y;
+        its.nit_all += it2.x;
+        its.kit_all += it2.y;
+        return st;
     }
     static __device__ __forceinline__ int step(WarpCtx<Cfg>& w, const R* y, R* ynew, R* delta, R* err,
                                                const R* drv, R* drv_new, R dt, R t, bool first_step,

@@ -106,6 +106,8 @@ class KernelSpec:
     # base, step start, BiCGSTAB shadow residual): "shared" memory of the
     # warp, or "local" (the lane's registers, spilling to local memory)
     scratch_placement: str = "shared"
+    # register cap per thread passed to the compiler (0: its default)
+    max_registers: int = 0
 
     @property
     def adaptive(self) -> bool:
@@ -426,7 +428,8 @@ def _generate_warp_kernel(system: SymbolicODE, spec: KernelSpec, gen: GeneratedS
         raise ValueError("block size must be a multiple of 32")
     warp_code = warp_code or generate_warp_system(system)
     spec = replace(spec, dense_prediction=False)
-    lines = ["// generated by cubie_b200.kernelgen (warp-per-system layout); do not edit"]
+    lines = ["// generated by cubie_b200.kernelgen (warp-per-system layout); do not edit",
+             f"// register cap: {int(spec.max_registers)}"]
     lines += DEVICE_INCLUDES
     lines.append('#include "cbx_warp.cuh"')
     lines.append("namespace cbxsys {")

@@ -57,7 +57,7 @@ LOOP_KEYS = {"save_every", "summarise_every", "sample_summaries_every"}
 DIRECT_MAX_WIDTH = 16
 EXECUTION_KEYS = {"mixed_precision", "kernel", "block_size", "min_blocks_per_sm", "max_steps", "device", "fast_math",
                   "precision", "adjoint", "layout", "schedule", "mem_proportion", "host_spill_threshold",
-                  "spill_dir", "max_chunk_runs", "scratch_placement"}
+                  "spill_dir", "max_chunk_runs", "scratch_placement", "max_registers"}
 IGNORED_KEYS = {"memory_settings", "cache", "auto_memory", "lineinfo", "time_logging_level",
                 "profileCUDA", "cache_settings"}
 RENAMED = {"dt_save": "save_every", "dt_summarise": "summarise_every",
@@ -153,6 +153,9 @@ class Solver:
             raise ValueError("scratch_placement must be 'shared', 'local' or 'auto'")
         self.placement_pending = sp_ == "auto"
         self.scratch_placement = "shared" if sp_ == "auto" else sp_
+        # register cap per thread for the compiler (0: its default); the
+        # warp layout's out-of-line stage solve otherwise stays at 128
+        self.max_registers = int(execution.get("max_registers", 0))
         # claim order of persistent launches: "auto" / "longest_first" sort
         # runs by decreasing per-run horizon when horizons are given
         self.schedule = str(execution.get("schedule", "auto"))
@@ -409,7 +412,7 @@ class Solver:
             mixed_precision=self.mixed_precision, block_size=self.block_size,
             min_blocks_per_sm=self.min_blocks_per_sm, adjoint=self.adjoint, layout=self.layout,
             dense_prediction=None if self.attempt_dense_prediction else False,
-            scratch_placement=self.scratch_placement,
+            scratch_placement=self.scratch_placement, max_registers=self.max_registers,
         )
 
     def _generate(self, spec: KernelSpec):
@@ -439,7 +442,10 @@ class Solver:
         key = (gk.key, self.device)
         mod = _MODULE_CACHE.get(key)
         if mod is None:
-            cubin, log = _native.compile_cubin(gk.source, _native.default_options(fast_math=self.fast_math))
+            opts = _native.default_options(fast_math=self.fast_math)
+            if spec.max_registers:
+                opts.append(f"--maxrregcount={int(spec.max_registers)}")
+            cubin, log = _native.compile_cubin(gk.source, opts)
             mod = _native.Module(cubin, self.device, log)
             _MODULE_CACHE[key] = mod
         return mod, gk
@@ -575,6 +581,8 @@ class Solver:
             self.block_size, self.min_blocks_per_sm = int(tuned["block"]), int(tuned["min_blocks"])
             if tuned.get("placement"):
                 self.scratch_placement = tuned["placement"]
+            if tuned.get("max_registers") is not None:
+                self.max_registers = int(tuned["max_registers"])
             self.autotune_result = tuned
             self.autotune_pending = self.placement_pending = False
             self.__dict__["_prepared"] = {}

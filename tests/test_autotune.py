@@ -67,16 +67,16 @@ def test_warp_layout_tunes_scratch_placement(tmp_path, monkeypatch):
                output_types=["state"])
     assert s.placement_pending and s.scratch_placement == "shared"
     cands = default_candidates(s)
-    assert {c[2] for c in cands} == {"shared", "local"} and all(len(c) == 3 for c in cands)
+    assert {c[2] for c in cands} == {"shared", "local"} and all(len(c) == 4 for c in cands)
     seen = []
 
     def fake(v):
-        seen.append((v.block_size, v.scratch_placement))
-        return 5.0 if (v.block_size, v.scratch_placement) == (64, "local") else 9.0
+        seen.append((v.block_size, v.scratch_placement, v.max_registers))
+        return 5.0 if (v.block_size, v.scratch_placement, v.max_registers) == (64, "local", 168) else 9.0
 
     r = autotune(s, None, None, 2.0, candidates=cands, timer=fake)
-    assert (r["block"], r["placement"], r["cached"]) == (64, "local", False)
-    assert sorted(seen) == sorted((c[0], c[2]) for c in cands)
+    assert (r["block"], r["placement"], r["max_registers"], r["cached"]) == (64, "local", 168, False)
+    assert sorted(seen) == sorted((c[0], c[2], c[3]) for c in cands)
     assert autotune(s, None, None, 2.0, candidates=cands, timer=fake)["cached"]
     # the placement is part of the generated source, not of the cache key
     fixed = Solver(sysm, algorithm="l_stable_dirk_3", layout="warp", scratch_placement="local",
