@@ -511,6 +511,7 @@ def cable_arm(args, dev, peak_fp32=None):
     drv = {"driver_sample_period": 0.01, "t0": 0.0, "order": 3, "wrap": False, "I": np.where(t_s < 5.0, 10.0, 0.0)}
     kw = dict(algorithm="l_stable_dirk_3", linear_correction_type="bicgstab", layout="warp", dt=0.025,
               scratch_placement=args.c3_placement, max_registers=args.c3_max_registers,
+              block_size="auto" if args.c3_placement == "auto" else 128,
               output_types=["mean", "max", "peaks[3]"], summarise_every=T, sample_summaries_every=0.1,
               summarise_variables=[f"V{j:02d}" for j in range(nc)], device=dev.index, max_steps=100000)
     sys32 = create_ODE_system(eqs, states=states, parameters=params, drivers=drivers, precision=np.float32)
@@ -518,7 +519,11 @@ def cable_arm(args, dev, peak_fp32=None):
     # +-65 mV state rounds at ~4e-6): rtol = atol = 1e-4 on both solves
     kw.update(rtol=1e-4, atol=1e-4)
     s32 = Solver(sys32, mixed_precision=True, **kw)
-    s32.solve(x0[:, :64], p[:, :64], drivers=drv, duration=T, nan_error_trajectories=False)   # compile, warm
+    # compile and warm up; with --c3-placement auto the first solve tunes
+    # the launch (warps per block, scratch placement, register cap) on a
+    # sample of the batch
+    W = min(n, 8192)
+    s32.solve(x0[:, :W], p[:, :W], drivers=drv, duration=T, nan_error_trajectories=False)
     times = []
     for _ in range(args.c3_steps):
         r = s32.solve(torch.as_tensor(x0, device=dev).float(), torch.as_tensor(p, device=dev).float(),
@@ -526,7 +531,8 @@ def cable_arm(args, dev, peak_fp32=None):
         times.append(s32.last_kernel_ms)
     K = min(256, n)
     sys64 = create_ODE_system(eqs, states=states, parameters=params, drivers=drivers, precision=np.float64)
-    r64 = Solver(sys64, **kw).solve(x0[:, :K], p[:, :K], drivers=drv, duration=T, nan_error_trajectories=False)
+    r64 = Solver(sys64, **dict(kw, scratch_placement="local", block_size=128, max_registers=0)).solve(
+        x0[:, :K], p[:, :K], drivers=drv, duration=T, nan_error_trajectories=False)
     a, b = r.state_summaries[:, :, :K].astype(np.float64), r64.state_summaries
     mean_max = np.concatenate([a[:, 0::5], a[:, 1::5]], axis=1), np.concatenate([b[:, 0::5], b[:, 1::5]], axis=1)
     err = np.max(np.abs(mean_max[0] - mean_max[1]) / (1e-3 + 1e-4 * np.abs(mean_max[1])), axis=(0, 1))
@@ -558,7 +564,11 @@ def cable_arm(args, dev, peak_fp32=None):
             "unit": "systems/s", "status_ok_fraction": float(np.mean(r.status_codes == 0)),
             "matched_fraction_vs_fp64_same_method": frac,
             "summary_error_units_pct50_90_99": [float(np.percentile(err, q)) for q in (50, 90, 99)],
-            "totals": r.totals, "roofline": roof, "note": "error units: 1e-3 + 1e-4 |ref| on mean and max V"}
+            "totals": r.totals, "roofline": roof,
+            "launch": {"block": s32.block_size, "scratch_placement": s32.scratch_placement,
+                       "max_registers": s32.max_registers,
+                       "autotune_ms": getattr(s32, "autotune_result", {}).get("timings_ms")},
+            "note": "error units: 1e-3 + 1e-4 |ref| on mean and max V"}
 
 
 def _native_fp32_peak(dev) -> float:
@@ -888,7 +898,7 @@ def main():
     ap.add_argument("--c5-steps", type=int, default=2)
     ap.add_argument("--c3-n", type=int, default=65536, help="Hodgkin-Huxley cable leg size (0: skip)")
     ap.add_argument("--c3-steps", type=int, default=2)
-    ap.add_argument("--c3-placement", default="shared", choices=["shared", "local", "auto"],
+    ap.add_argument("--c3-placement", default="auto", choices=["shared", "local", "auto"],
                     help="stage-solve scratch placement of the cable's warp kernel")
     ap.add_argument("--c3-max-registers", type=int, default=0, help="register cap of the cable's warp kernel "
                     "(0: the compiler's default)")

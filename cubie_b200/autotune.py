@@ -124,6 +124,8 @@ def autotune(solver, inits, params, duration: float, durations=None, candidates:
         return dict(block=hit["block"], min_blocks=hit["min_blocks"], placement=hit.get("placement"),
                     max_registers=hit.get("max_registers"), timings_ms=hit["timings_ms"], cached=True)
     measure = timer or _gpu_timer(inits, params, duration, durations, repeats, interp)
+    if timer is None:
+        _precompile([variant(solver, *c) for c in cands], duration, durations, interp)
     timings = {}
     for shape in cands:
         try:
@@ -140,6 +142,36 @@ def autotune(solver, inits, params, duration: float, durations=None, candidates:
         tmp.write_text(json.dumps(store, indent=1, sort_keys=True))
         os.replace(tmp, path)
     return dict(result, cached=False)
+
+
+def _precompile(variants, duration, durations, interp) -> None:
+    """Compile every candidate at once on the host's cores (NVRTC releases
+    the interpreter lock), then load the modules one by one; the timing
+    loop then finds them loaded."""
+    from concurrent.futures import ThreadPoolExecutor
+    specs = []
+    for v in variants:
+        timing = v._timing(float(duration))
+        specs.append(v.kernel_spec(timing, interp.device_meta() if interp is not None else None))
+    if variants:
+        variants[0]._generate(specs[0])   # the symbolic part once, shared by every variant
+    workers = max(1, min(len(variants), os.cpu_count() or 1))
+
+    def build(pair):
+        v, spec = pair
+        try:
+            return v.compile_for(spec)
+        except Exception:  # the timing loop reports the candidate as failed
+            return None
+
+    with ThreadPoolExecutor(workers) as ex:
+        results = list(ex.map(build, zip(variants, specs)))
+    for v, spec, res in zip(variants, specs, results):
+        if res is not None:
+            try:
+                v.module_for(spec, compiled=res)
+            except Exception:
+                pass
 
 
 def _gpu_name(device: int) -> str:

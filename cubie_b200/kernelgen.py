@@ -105,7 +105,7 @@ class KernelSpec:
     # where the warp layout keeps its stage-solve scratch vectors (stage
     # base, step start, BiCGSTAB shadow residual): "shared" memory of the
     # warp, or "local" (the lane's registers, spilling to local memory)
-    scratch_placement: str = "shared"
+    scratch_placement: str = "local"
     # register cap per thread passed to the compiler (0: its default)
     max_registers: int = 0
 

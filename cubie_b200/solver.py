@@ -147,8 +147,9 @@ class Solver:
             raise ValueError("layout must be 'thread', 'warp' or 'auto'")
         self.layout = layout
         # warp layout: stage-solve scratch vectors in "shared" memory or
-        # "local" (registers / local memory); "auto" lets the autotuner pick
-        sp_ = str(execution.get("scratch_placement", "shared"))
+        # "local" (registers / local memory; the faster of the two on the
+        # 256-state cable); "auto" lets the autotuner pick
+        sp_ = str(execution.get("scratch_placement", "local"))
         if sp_ not in ("shared", "local", "auto"):
             raise ValueError("scratch_placement must be 'shared', 'local' or 'auto'")
         self.placement_pending = sp_ == "auto"
@@ -436,16 +437,28 @@ class Solver:
                 warp = cache["warp"] = generate_warp_system(self.system)
         return generate_kernel(self.system, spec, gen=gen, warp_code=warp)
 
-    def module_for(self, spec: KernelSpec):
-        """Compile (or fetch) the NVRTC module for ``spec`` on this device."""
+    def compile_for(self, spec: KernelSpec):
+        """NVRTC-compile ``spec`` (no device needed; safe to call from
+        several threads at once).  Returns ``(gk, cubin, log)``, or
+        ``(gk, None, None)`` when the module is already loaded."""
         gk = self._generate(spec)
+        if (gk.key, self.device) in _MODULE_CACHE:
+            return gk, None, None
+        opts = _native.default_options(fast_math=self.fast_math)
+        if spec.max_registers:
+            opts.append(f"--maxrregcount={int(spec.max_registers)}")
+        cubin, log = _native.compile_cubin(gk.source, opts)
+        return gk, cubin, log
+
+    def module_for(self, spec: KernelSpec, compiled=None):
+        """Compile (or fetch) the NVRTC module for ``spec`` on this device;
+        ``compiled`` is a result of :meth:`compile_for` to load instead."""
+        gk, cubin, log = compiled if compiled is not None else self.compile_for(spec)
         key = (gk.key, self.device)
         mod = _MODULE_CACHE.get(key)
         if mod is None:
-            opts = _native.default_options(fast_math=self.fast_math)
-            if spec.max_registers:
-                opts.append(f"--maxrregcount={int(spec.max_registers)}")
-            cubin, log = _native.compile_cubin(gk.source, opts)
+            if cubin is None:
+                gk, cubin, log = self.compile_for(spec)
             mod = _native.Module(cubin, self.device, log)
             _MODULE_CACHE[key] = mod
         return mod, gk
