@@ -10,7 +10,9 @@
 // persistent loop (lanes claim the family's next run the moment their run
 // ends), then moves on to the next family that still has runs; warps start
 // at different families (rotated by warp index) so all families progress
-// together and the launch ends when the last family's runs are done.  Each
+// together and the launch ends when the last family's runs are done.
+// Within a family, claims follow its run_order when one is given (longest
+// horizon first, as in the single-family persistent launch).  Each
 // family's loop is its own function instantiation with its own loop state,
 // so the registers a lane needs are the most any one family needs, not the
 // sum.
@@ -25,9 +27,9 @@ __device__ __forceinline__ void drain_family(const cbx_solve_args& a, unsigned l
     bool active = false, exhausted = false;
     while (true) {
         if (!active && !exhausted) {
-            const long long run = claim_run(counter);
-            if (run < a.n_runs) {
-                lane_begin<Cfg>(L, a, run);
+            const long long k = claim_run(counter);
+            if (k < a.n_runs) {
+                lane_begin<Cfg>(L, a, a.run_order ? a.run_order[k] : k);
                 active = true;
             } else {
                 exhausted = true;

@@ -48,7 +48,9 @@ struct Lane {
     int save_idx, summary_idx, update_idx;
     int status, iteration_status, stagnant;
     bool first_step, prev_accepted, irrecoverable;
-    long long steps, rejections, newton, krylov;
+    // per-run totals, 32-bit (a run of more than 2^32 attempted steps would
+    // wrap them; the launch totals are 64-bit)
+    unsigned steps, rejections, newton, krylov;
     typename Ctl::State ctl;
     typename Step::Persist ps;
 };
@@ -255,7 +257,7 @@ __device__ __forceinline__ bool lane_iterate(Lane<Cfg>& L, const cbx_solve_args 
     // (reserved but unused in the reference, result_codes.py:57).  Written
     // as direct returns: folding them into ``irrecoverable`` ahead of the
     // finish test made NVRTC's optimiser drop the event clamp below.
-    if (a.max_steps > 0 && L.steps >= a.max_steps) {
+    if (a.max_steps > 0 && (long long)L.steps >= a.max_steps) {
         L.status |= MAX_LOOP_ITERS_EXCEEDED;
         return true;
     }

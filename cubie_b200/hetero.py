@@ -28,19 +28,84 @@ from .solver import Solver, _is_tensor, _torch
 _HETERO_MODULES: Dict[tuple, "_native.Module"] = {}
 
 
-class HeteroSolver:
-    """One launch over the runs of several solvers."""
+# Relative tolerance below which FP32 stepping cannot honour a run's
+# tolerance: an FP32 state carries about 6e-8 relative rounding per
+# operation, and the reference's own gate rejects FP32 results below about
+# 1e-6 (tests/integrated_numerical_tests/julia_reference/ne_gate.py:38-41).
+FP32_RTOL_FLOOR = 1e-6
 
-    def __init__(self, solvers: Sequence[Solver], block_size: Optional[int] = None):
+
+def _take(x, idx):
+    """Columns ``idx`` (runs) of an array or tensor ``[..., n]``."""
+    if x is None:
+        return None
+    if _is_tensor(x):
+        torch = _torch()
+        return x.index_select(x.dim() - 1, torch.as_tensor(idx, device=x.device, dtype=torch.long))
+    return np.asarray(x)[..., idx]
+
+
+class HeteroSolver:
+    """One launch over the runs of several solvers.
+
+    ``fp32_floor``: runs of an FP32 (or mixed-precision) family whose
+    tightest relative tolerance (``rtol`` x the run's ``tol_scale``) lies
+    below it are integrated by an FP64-stepping twin of that family, added
+    to the same launch; the family's results come back merged in the
+    caller's run order (in FP64 when any run was routed).  ``None`` turns
+    the routing off."""
+
+    def __init__(self, solvers: Sequence[Solver], block_size: Optional[int] = None,
+                 fp32_floor: Optional[float] = FP32_RTOL_FLOOR):
         if not 1 <= len(solvers) <= _native.HeteroArgs.MAX_FAMILIES:
             raise ValueError(f"one to {_native.HeteroArgs.MAX_FAMILIES} solvers per launch")
         devices = {s.device for s in solvers}
         if len(devices) != 1:
             raise ValueError("all solvers must use the same device")
+        self.user_solvers = list(solvers)
         self.solvers = list(solvers)
         self.device = devices.pop()
         self.block_size = int(block_size or solvers[0].block_size)
+        self.fp32_floor = fp32_floor
         self.last_kernel_ms = None
+        self._twins: Dict[int, Solver] = {}
+
+    def route(self, batches: Sequence[Dict[str, Any]]):
+        """Split each FP32 family's batch at the floor: returns the launch's
+        (solver, batch) families and, per caller family, a list of
+        ``(launch family, run indices)``."""
+        fams, routes = [], []
+        for k, (s, b) in enumerate(zip(self.user_solvers, batches)):
+            iv = b["initial_values"]
+            n = int(iv.shape[1]) if hasattr(iv, "shape") and len(iv.shape) == 2 else None
+            low = None
+            if self.fp32_floor is not None and s.precision == np.float32 and n is not None:
+                ts = b.get("tol_scale")
+                scale = np.ones(n) if ts is None else np.asarray(
+                    ts.detach().cpu().numpy() if _is_tensor(ts) else ts, dtype=np.float64).reshape(-1)
+                low = float(np.min(s.rtol)) * scale < self.fp32_floor
+            if low is None or not low.any():
+                routes.append([(len(fams), None)])
+                fams.append((s, b))
+                continue
+            hi_idx, lo_idx = np.where(~low)[0], np.where(low)[0]
+            twin = self._twins.get(k)
+            if twin is None:
+                twin = self._twins[k] = s.with_precision(np.float64)
+            route = []
+            for solver, idx in ((s, hi_idx), (twin, lo_idx)):
+                if idx.size == 0:
+                    continue
+                sub = dict(b)
+                for key in ("initial_values", "parameters", "durations", "tol_scale"):
+                    if b.get(key) is not None:
+                        sub[key] = _take(b[key], idx)
+                route.append((len(fams), idx))
+                fams.append((solver, sub))
+            routes.append(route)
+        if len(fams) > _native.HeteroArgs.MAX_FAMILIES:
+            raise ValueError(f"{len(fams)} families after FP64 routing; at most {_native.HeteroArgs.MAX_FAMILIES}")
+        return fams, routes
 
     def _module(self, preps):
         fams = []
@@ -65,8 +130,11 @@ class HeteroSolver:
         torch = _torch()
         if not torch.cuda.is_available():
             raise RuntimeError("cubie_b200 needs a CUDA device: no GPU is visible")
-        if len(batches) != len(self.solvers):
+        if len(batches) != len(self.user_solvers):
             raise ValueError("one batch per solver")
+        fams, routes = self.route(batches)
+        self.solvers = [f[0] for f in fams]
+        batches = [f[1] for f in fams]
         dev = torch.device("cuda", self.device)
         preps, bufs, args, keep = [], [], [], []
         first = [0]
@@ -87,8 +155,11 @@ class HeteroSolver:
             dt = None if durs is None else torch.as_tensor(durs).to(device=dev, dtype=torch.float64).contiguous()
             ts = b.get("tol_scale")
             tt = None if ts is None else torch.as_tensor(ts).to(device=dev, dtype=torch.float64).contiguous()
+            # runs claimed longest horizon first within each family
+            order = s.run_order(dt) if dt is not None else None
             a = s.make_args(prep, bf, it, pt, None, n, duration, b.get("settling_time", 0.0), b.get("t0", 0.0),
-                            dt, tt)
+                            dt, tt, order_t=order)
+            keep.append(order)
             preps.append(prep)
             bufs.append(bf)
             args.append(a)
@@ -106,7 +177,9 @@ class HeteroSolver:
         per_sm = mod.occupancy(2, self.block_size)
         sms = _native.device_info(self.device)["sm_count"]
         grid = max(1, min(max(per_sm, 1) * sms, (first[-1] + self.block_size - 1) // self.block_size))
-        return HeteroLaunch(self, batches, mod, h, work, preps, bufs, keep, grid)
+        launch = HeteroLaunch(self, batches, mod, h, work, preps, bufs, keep, grid)
+        launch.routes = routes
+        return launch
 
     def solve(self, batches: Sequence[Dict[str, Any]], nan_error_trajectories: bool = True,
               on_device: bool = False, stream=None) -> List:
@@ -162,9 +235,47 @@ class HeteroLaunch:
         return g
 
     def collect(self, nan_error_trajectories: bool = True, on_device: bool = False) -> List:
-        out = []
+        """One SolveResult per caller family, in the caller's run order."""
+        per_launch = []
         for s, b, prep, bf in zip(self.owner.solvers, self.batches, self.preps, self.bufs):
             s.last_kernel_ms = self.owner.last_kernel_ms
-            out.append(s.collect(prep, bf, int(bf["status"].shape[0]), float(b["duration"]),
-                                 b.get("settling_time", 0.0), b.get("t0", 0.0), nan_error_trajectories, on_device))
+            per_launch.append(s.collect(prep, bf, int(bf["status"].shape[0]), float(b["duration"]),
+                                        b.get("settling_time", 0.0), b.get("t0", 0.0), nan_error_trajectories,
+                                        on_device))
+        routes = getattr(self, "routes", None) or [[(k, None)] for k in range(len(per_launch))]
+        out = []
+        for route in routes:
+            if len(route) == 1 and route[0][1] is None:
+                out.append(per_launch[route[0][0]])
+            else:
+                if on_device:
+                    raise ValueError("routed families are merged on the host (on_device=False)")
+                out.append(merge_results([(per_launch[f], idx) for f, idx in route]))
         return out
+
+
+def merge_results(parts) -> "SolveResult":
+    """Reassemble one family's SolveResult from sub-results over disjoint run
+    index sets ``[(result, run_indices), ...]`` (arrays promoted to the
+    widest dtype among the parts; totals summed)."""
+    import copy
+    first = parts[0][0]
+    n = sum(len(idx) for _, idx in parts)
+    res = copy.copy(first)
+    for name in ("state", "observables", "state_summaries", "observable_summaries", "iteration_counters"):
+        arrs = [getattr(r, name) for r, _ in parts]
+        if any(a is None for a in arrs):
+            setattr(res, name, None)
+            continue
+        dtype = np.result_type(*arrs)
+        full = np.empty(arrs[0].shape[:-1] + (n,), dtype=dtype)
+        for a, (_, idx) in zip(arrs, parts):
+            full[..., idx] = a
+        setattr(res, name, full)
+    status = np.empty(n, dtype=first.status_codes.dtype)
+    for r, idx in parts:
+        status[idx] = r.status_codes
+    res.status_codes = status
+    if all(r.totals is not None for r, _ in parts):
+        res.totals = {k: sum(r.totals[k] for r, _ in parts) for k in first.totals}
+    return res

@@ -808,6 +808,19 @@ class Solver:
             res.mask_error_runs()
         return res
 
+    def with_precision(self, precision) -> "Solver":
+        """A solver with the same settings stepping the same system at
+        ``precision`` throughout (no mixed precision)."""
+        import copy
+        twin = copy.copy(self)
+        twin.system = self.system.with_precision(precision)
+        twin.precision = np.dtype(precision).type
+        twin.mixed_precision = False
+        for key in ("_system_code", "_prepared"):
+            twin.__dict__.pop(key, None)
+        twin._modules = {}
+        return twin
+
     def close(self) -> None:
         pass
 

@@ -204,6 +204,13 @@ class SymbolicODE:
         self.observable_symbols = [sp.Symbol(n, real=True) for n in self.observable_names]
         self._jac = None
 
+    def with_precision(self, precision) -> "SymbolicODE":
+        """The same system compiled at another precision."""
+        return SymbolicODE(states=self.initial_values, parameters=self.parameters, constants=self.constants,
+                           drivers=self.driver_names, observables=self.observable_names,
+                           assignments=self.assignments, derivatives=self.derivatives, precision=precision,
+                           name=self.name, driver_settings=self.driver_settings, source=self._source)
+
     # -- sizes ---------------------------------------------------------
     @property
     def num_states(self) -> int:

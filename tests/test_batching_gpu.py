@@ -121,3 +121,26 @@ def test_chunked_solve_equals_unchunked(cuda_device, tmp_path, per_run_horizons)
             np.testing.assert_array_equal(res.state_summaries, whole.state_summaries)
         np.testing.assert_array_equal(res.iteration_counters, whole.iteration_counters)
         assert res.totals == whole.totals
+
+
+def test_fp32_floor_routing_matches_separate_solves(cuda_device):
+    """A mixed-precision family with per-run tolerances straddling the FP32
+    floor: the runs below it come back from the FP64 twin family of the same
+    launch, bit-identical to an FP64 solve of those runs, the others
+    bit-identical to the mixed-precision solve, in the caller's order."""
+    from test_hetero_emulated import families
+    from cubie_b200.hetero import FP32_RTOL_FLOOR, HeteroSolver
+    solvers, batches = families()
+    ts = np.array([1.0, 1e-3, 1.0, 1e-2, 0.5, 1.0, 1e-4])
+    batches[1] = dict(batches[1], tol_scale=ts)
+    hs = HeteroSolver(solvers)
+    results = hs.solve(batches, nan_error_trajectories=False)
+    s, b, r = solvers[1], batches[1], results[1]
+    low = 1e-6 * ts < FP32_RTOL_FLOOR
+    assert r.state.dtype == np.float64 and r.status_codes.shape == (7,)
+    for mask, solver in ((low, s.with_precision(np.float64)), (~low, s)):
+        idx = np.where(mask)[0]
+        ref = solver.solve(b["initial_values"][:, idx], b["parameters"][:, idx], duration=b["duration"],
+                           durations=b["durations"][idx], tol_scale=ts[idx], nan_error_trajectories=False)
+        assert r.status_codes[idx].tolist() == ref.status_codes.tolist()
+        np.testing.assert_array_equal(r.state[..., idx], ref.state.astype(np.float64))

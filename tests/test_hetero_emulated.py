@@ -45,3 +45,28 @@ def test_hetero_equals_separate_solves():
         assert o["status"].tolist() == ref["status"].tolist()
         np.testing.assert_array_equal(o["state"], ref["state"])
         assert o["totals"].tolist() == ref["totals"].tolist()
+
+
+def test_fp32_floor_routes_tight_runs_to_an_fp64_twin():
+    """Runs of an FP32 family whose rtol x tol_scale lies below the FP32
+    floor go to an FP64 twin family in the same launch (CPU: the routing
+    only)."""
+    from cubie_b200.hetero import FP32_RTOL_FLOOR, HeteroSolver
+    solvers, batches = families()
+    ts = np.array([1.0, 1e-3, 1.0, 1e-2, 0.5, 1.0, 1e-4])     # VdP rtol 1e-6 x scale
+    batches[1] = dict(batches[1], tol_scale=ts)
+    hs = HeteroSolver(solvers)
+    fams, routes = hs.route(batches)
+    low = np.where(1e-6 * ts < FP32_RTOL_FLOOR)[0]
+    assert low.tolist() == [1, 3, 4, 6]
+    assert len(fams) == 4 and len(routes[1]) == 2
+    (f_hi, hi), (f_lo, lo) = routes[1]
+    assert lo.tolist() == low.tolist() and sorted(hi.tolist() + lo.tolist()) == list(range(7))
+    twin, sub = fams[f_lo]
+    assert twin.precision == np.float64 and not twin.mixed_precision
+    assert twin.algorithm == solvers[1].algorithm and twin.system.state_names == solvers[1].system.state_names
+    np.testing.assert_array_equal(sub["initial_values"], batches[1]["initial_values"][:, low])
+    np.testing.assert_array_equal(sub["tol_scale"], ts[low])
+    # the FP64 family (Robertson) and families without tight runs are untouched
+    assert routes[0] == [(0, None)] and routes[2] == [(3, None)]
+    assert HeteroSolver(solvers, fp32_floor=None).route(batches)[1][1] == [(1, None)]
