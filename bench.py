@@ -370,11 +370,18 @@ def hetero_arm(args, dev):
     by default); per-run rtol = 10^U[-8,-4] (a per-run scale on rtol 1e-4),
     per-run horizon 10^U[0,3]; FP32 stepping with FP64 time, control and
     norms; final state only; one heterogeneous persistent launch replayed as
-    a CUDA graph.  Solved: status 0, and for Van der Pol and Robertson the
-    final state within 10 tolerance units (of that run's rtol) of an FP64
-    Radau solve at rtol 1e-11 on 512 runs per system; Lorenz runs are
-    checked by status only (the final state of a chaotic run over hundreds
-    of time units has no tolerance-scale reference)."""
+    a CUDA graph.  Runs whose rtol lies below the FP32 floor (1e-6) go to
+    FP64-stepping twins of their family inside the same launch; the same
+    launch without that routing is timed beside it.  Solved: status 0, and
+    for Van der Pol and Robertson the final state within 10 tolerance units
+    (of that run's rtol) of an FP64 Radau solve at rtol 1e-11 on 512 runs
+    per system; Lorenz runs are checked by status only (the final state of a
+    chaotic run over hundreds of time units has no tolerance-scale
+    reference).  After the launch, the Lorenz family's discrete adjoint:
+    loss = mean squared error of its states saved every 1.0 over t in
+    [0, 10] against seeded targets, gradients with respect to the initial
+    states and rho, the family's per-run tolerances, FP32 stepping with FP64
+    control."""
     import torch
     from cubie_b200 import Solver, create_ODE_system, _native
     from cubie_b200.hetero import HeteroSolver
@@ -404,24 +411,35 @@ def hetero_arm(args, dev):
                             parameters=torch.as_tensor(p, device=dev).float(),
                             duration=float(horizon.max()), durations=horizon, tol_scale=rtol / 1e-4,
                             _rtol=rtol, _x0=x0, _p=p))
-    hs = HeteroSolver(solvers)
-    run = hs.setup(batches)
-    graph = run.graph()
     stream = torch.cuda.current_stream(dev)
     flush = torch.empty(int(256e6) // 4, dtype=torch.int32, device=dev)
-    times = []
-    for it in range(1 + args.c5_steps):
-        _native.flush_l2(flush.data_ptr(), flush.numel() * 4, stream.cuda_stream)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        graph.replay()
-        e1.record(stream)
-        e1.synchronize()
-        if it >= 1:
-            times.append(e0.elapsed_time(e1))
-    del graph
-    hs.last_kernel_ms = float(np.mean(times))
+
+    def timed(hs, steps):
+        run = hs.setup(batches)
+        graph = run.graph()
+        times = []
+        for it in range(1 + steps):
+            _native.flush_l2(flush.data_ptr(), flush.numel() * 4, stream.cuda_stream)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            graph.replay()
+            e1.record(stream)
+            e1.synchronize()
+            if it >= 1:
+                times.append(e0.elapsed_time(e1))
+        del graph
+        hs.last_kernel_ms = float(np.mean(times))
+        return run, times
+
+    hs = HeteroSolver(solvers)
+    run, times = timed(hs, args.c5_steps)
     results = run.collect(nan_error_trajectories=False)
+    routed = {name: int(sum(len(idx) for f, idx in rt[1:])) if len(rt) > 1 else 0
+              for name, rt in zip(("lorenz", "vdp", "robertson"), run.routes)}
+    plain_hs = HeteroSolver(solvers, fp32_floor=None)
+    plain_run, plain_times = timed(plain_hs, 1)
+    plain_res = plain_run.collect(nan_error_trajectories=False)
+    del plain_run
     fam = {}
     solved_total = 0.0
     for name, s64sys, b, r in (("lorenz", None, batches[0], results[0]),
@@ -445,19 +463,75 @@ def hetero_arm(args, dev):
             err = np.max(np.abs(y - yt) / (atol + b["_rtol"][None, :T] * np.abs(yt)), axis=0)
             good = (tr.status_codes == 0)
             frac = float(np.sum(ok[:T] & good & (err <= SOLVED_TOL_UNITS)) / max(1, np.sum(good)))
+            # the same runs from the launch without FP64 routing
+            pr = plain_res[1 if name == "vdp" else 2]
+            yp = pr.state[-1][:, :T].astype(np.float64)
+            errp = np.max(np.abs(yp - yt) / (atol + b["_rtol"][None, :T] * np.abs(yt)), axis=0)
+            fracp = float(np.sum((pr.status_codes[:T] == 0) & good & (errp <= SOLVED_TOL_UNITS)) /
+                          max(1, np.sum(good)))
             fam[name] = {"solved_fraction": frac, "status_ok_fraction": float(np.mean(ok)),
                          "error_tol_units_pct50_90_99": [float(np.percentile(err[good], q)) for q in (50, 90, 99)],
+                         "routed_to_fp64": routed[name], "solved_fraction_without_routing": fracp,
                          "totals": r.totals}
         else:
-            fam[name] = {"solved_fraction": frac, "status_ok_fraction": frac, "totals": r.totals}
+            fam[name] = {"solved_fraction": frac, "status_ok_fraction": frac, "routed_to_fp64": routed[name],
+                         "totals": r.totals}
         solved_total += n * fam[name]["solved_fraction"]
     ms = float(np.mean(times))
+    adj = c5_lorenz_adjoint(args, dev, solvers[0], batches[0], stream, flush)
     del flush
     return {"workload": f"2^20 runs split evenly: Lorenz DP54, stiff VdP ROS3P, Robertson ROS3P (stage systems: "
                         f"{args.linear}); per-run rtol 10^U[-8,-4], per-run horizon 10^U[0,3]; FP32 stepping + FP64 "
                         f"control; one heterogeneous persistent launch replayed as a CUDA graph",
             "n_systems": 3 * n, "ms": ms, "value": solved_total / (ms * 1e-3), "unit": "systems/s",
-            "families": fam, "graph": True}
+            "families": fam, "graph": True, "fp32_floor": hs.fp32_floor,
+            "without_routing": {"ms": float(np.mean(plain_times)),
+                                "vdp_solved_fraction": fam["vdp"]["solved_fraction_without_routing"]},
+            "lorenz_adjoint": adj}
+
+
+def c5_lorenz_adjoint(args, dev, lor_solver, batch, stream, flush):
+    """Discrete adjoint of the mixed batch's Lorenz family over a bounded
+    window: its own inputs and per-run tolerance scales, states saved every
+    1.0 over t in [0, 10], loss = mean((y - target)^2) with seeded targets.
+    Forward with checkpoints every 64 accepted steps plus the reverse sweep,
+    timed with CUDA events (one warm-up pass)."""
+    import torch
+    from cubie_b200 import Solver
+    from cubie_b200.adjoint import AdjointIntegrator
+    T = 10.0
+    solver = Solver(lor_solver.system, algorithm="dormand-prince-54", rtol=1e-4, atol=1e-8,
+                    output_types=["state"], save_every=1.0, mixed_precision=True, adjoint=True, device=dev.index)
+    n = int(batch["initial_values"].shape[1])
+    rng = np.random.default_rng(55)
+    target = torch.as_tensor(rng.uniform(-10.0, 10.0, (int(T) + 1, 3, n)), device=dev, dtype=torch.float32)
+    integ = AdjointIntegrator(solver, ckpt_every=64, max_ckpts=128)
+    ts = np.asarray(batch["tol_scale"], dtype=np.float64)
+    fwd_ms, tot_ms = [], []
+    for it in range(2):
+        _native_flush(flush, stream)
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        e0.record(stream)
+        state, status, saved = integ.forward(batch["initial_values"], batch["parameters"], T, tol_scale=ts)
+        e1.record(stream)
+        grad = (2.0 / target.numel()) * (state - target)
+        gi, gp = integ.backward(saved, grad)
+        e2.record(stream)
+        e2.synchronize()
+        if it == 1:
+            fwd_ms.append(e0.elapsed_time(e1))
+            tot_ms.append(e0.elapsed_time(e2))
+    st = status.cpu().numpy()
+    return {"n_systems": n, "window": "t in [0, 10], saved every 1.0", "fwd_ms": fwd_ms[0],
+            "fwd_plus_adjoint_ms": tot_ms[0], "ratio": tot_ms[0] / fwd_ms[0],
+            "status_ok_fraction": float(np.mean(st == 0)),
+            "grad_finite_fraction": float(torch.isfinite(gi).all(dim=0).float().mean().item()),
+            "checkpoint_and_record_bytes": list(integ.sizes(saved["prep"]))}
+
+
+def _native_flush(flush, stream):
+    from cubie_b200 import _native
+    _native.flush_l2(flush.data_ptr(), flush.numel() * 4, stream.cuda_stream)
 
 
 def hh_cable(nc):

@@ -75,7 +75,7 @@ class AdjointIntegrator:
             adj.tape, adj.tape_flags, adj.step_count = (t.data_ptr() for t in tape)
 
     def forward(self, inits_t, params_t, duration: float, settling_time: float = 0.0, t0: float = 0.0,
-                stream=None):
+                stream=None, tol_scale=None):
         """Integrate with checkpoints.  Returns ``(state, status, saved)``:
         the saved-state tensor ``[rows, n_saved (+time), n_runs]`` on the
         device, the status words and the context :meth:`backward` needs."""
@@ -95,7 +95,9 @@ class AdjointIntegrator:
         st.wait_stream(torch.cuda.current_stream(dev))
         with torch.cuda.stream(st):
             bufs = s.allocate_outputs(prep, n_runs, dev, tdtype)
-            args = s.make_args(prep, bufs, inits_t, params_t, None, n_runs, duration, settling_time, t0)
+            tol_t = None if tol_scale is None else torch.as_tensor(tol_scale).to(device=dev, dtype=torch.float64)
+            args = s.make_args(prep, bufs, inits_t, params_t, None, n_runs, duration, settling_time, t0,
+                               None, tol_t)
         lane, record, tape_entry = self.sizes(prep)
         words = lane // 4
         with torch.cuda.stream(st):
@@ -110,7 +112,8 @@ class AdjointIntegrator:
         adj.max_ckpts = self.max_ckpts
         self._set_tape(adj, tape)
         prep["module"].adjoint_launch(args, adj, 0, s.block_size, 0, st.cuda_stream)
-        saved = dict(prep=prep, bufs=bufs, inits=inits_t, params=params_t, ckpt=ckpt, count=count, words=words,
+        saved = dict(prep=prep, bufs=bufs, inits=inits_t, params=params_t, tol=tol_t, ckpt=ckpt, count=count,
+                     words=words,
                      record=record, tape=tape,
                      n_runs=n_runs, duration=duration, settling_time=settling_time, t0=t0, dev=dev, tdtype=tdtype)
         return bufs["state"], bufs["status"], saved
@@ -136,7 +139,7 @@ class AdjointIntegrator:
             gi = torch.empty((n, n_runs), device=dev, dtype=tdtype)
             gp = torch.empty((max(npar, 1), n_runs), device=dev, dtype=tdtype)
             args = s.make_args(prep, bufs, saved["inits"], saved["params"], None, n_runs, saved["duration"],
-                               saved["settling_time"], saved["t0"])  # zeroes the work counter
+                               saved["settling_time"], saved["t0"], None, saved["tol"])  # zeroes the work counter
         adj = _native.AdjointArgs()
         adj.ckpt = saved["ckpt"].data_ptr()
         adj.ckpt_count = saved["count"].data_ptr()

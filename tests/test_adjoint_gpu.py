@@ -134,3 +134,44 @@ def test_checkpoint_capacity_exhaustion_sets_status_32(cuda_device):
     integ = AdjointIntegrator(solver, ckpt_every=2, max_ckpts=3)
     state, status, _ = integ.forward(torch.tensor(x0, device="cuda"), torch.tensor(p, device="cuda"), 20.0)
     assert np.all(status.cpu().numpy() == 32)
+
+
+LORENZ = ["dx = sigma * (y - x)", "dy = x * (rho - z) - y", "dz = x * y - beta * z"]
+
+
+def test_lorenz_adjoint_with_per_run_tolerances(cuda_device):
+    """The adjoint of the mixed three-system batch's Lorenz family: DP54 with
+    FP32 stepping and FP64 control, per-run tolerance scales (rtol from 1e-7
+    to 1e-5, as the batch draws them), loss = mean squared error of every
+    saved state over a bounded window (t in [0, 2], saved every 0.25)
+    against seeded targets.  Gradients with respect to the initial states
+    and rho against the FP64 forward sensitivities."""
+    import torch
+    from cubie_b200 import Solver, create_ODE_system
+    from cubie_b200.adjoint import AdjointIntegrator
+    from oracle.sensitivity import SensitivitySystem, trajectory_gradients
+    n, T, every = 16, 2.0, 0.25
+    rng = np.random.default_rng(21)
+    rho = rng.uniform(20.0, 35.0, n)
+    x0 = rng.uniform(-10.0, 10.0, (3, n))
+    ts = 10.0 ** rng.uniform(-2.0, 0.0, n)
+    rows = int(round(T / every)) + 1
+    target = rng.uniform(-10.0, 10.0, (rows, 3, n))
+    consts = {"sigma": 10.0, "beta": 8.0 / 3.0}
+    sysm = create_ODE_system(LORENZ, states={"x": 1.0, "y": 0.0, "z": 0.0}, parameters={"rho": 21.0},
+                             constants=consts, precision=np.float32)
+    solver = Solver(sysm, algorithm="dormand-prince-54", rtol=1e-5, atol=1e-7, output_types=["state"],
+                    save_every=every, mixed_precision=True, adjoint=True)
+    integ = AdjointIntegrator(solver, ckpt_every=64, max_ckpts=64)
+    xi = torch.tensor(x0, device="cuda", dtype=torch.float32)
+    pi = torch.tensor(rho[None, :], device="cuda", dtype=torch.float32)
+    state, status, saved = integ.forward(xi, pi, T, tol_scale=ts)
+    assert status.cpu().numpy().tolist() == [0] * n
+    s_np = state.double().cpu().numpy()
+    g_rows = 2.0 * (s_np - target) / target.size
+    gi, gp = integ.backward(saved, torch.tensor(g_rows, device="cuda", dtype=torch.float32))
+    ssys = SensitivitySystem(LORENZ, ["x", "y", "z"], ["rho"], consts)
+    _, gy0, gpr = trajectory_gradients(ssys, x0, rho[None, :], np.arange(rows) * every, g_rows,
+                                       rtol=1e-11, atol=1e-11)
+    assert _rel(gi.double().cpu().numpy(), gy0) < 5e-3
+    assert _rel(gp.double().cpu().numpy(), gpr) < 5e-3

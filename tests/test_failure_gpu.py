@@ -44,3 +44,38 @@ def test_nonfinite_inputs_fail_and_are_masked(cuda_device):
     assert res.status_codes[1] != 0 and res.status_codes[2] != 0
     assert np.all(np.isnan(res.state[..., 1])) and np.all(np.isnan(res.state[..., 2]))
     assert np.all(np.isfinite(res.state[..., 0]))
+
+
+def test_abort_flag_raised_while_the_launch_runs(cuda_device):
+    """The host raises the abort flag while a long persistent launch runs
+    (stiff runs with the reference's default minimal-residual stage solves
+    take seconds each): the launch ends early, the runs still going end
+    with status bit 32, and the runs already finished keep status 0."""
+    import time
+    import torch
+    solver = _solver(max_steps=200_000)
+    n = 4096
+    rng = np.random.default_rng(5)
+    dev = torch.device("cuda", cuda_device)
+    mu = 10 ** rng.uniform(0.0, 3.0, n)
+    prep = solver.prepare(2000.0, durations=2.0 * mu)
+    inits = torch.as_tensor(rng.uniform(-2, 2, (2, n)), device=dev).float()
+    params = torch.as_tensor(mu[None, :], device=dev).float()
+    durs = torch.as_tensor(2.0 * mu, device=dev, dtype=torch.float64)
+    bufs = solver.allocate_outputs(prep, n, dev, torch.float32)
+    flag = torch.zeros((1,), dtype=torch.int32).pin_memory()    # host memory the kernel polls
+    args = solver.make_args(prep, bufs, inits, params, None, n, 2000.0, 0.0, 0.0, durs)
+    args.abort_flag = flag.data_ptr()
+    stream = torch.cuda.current_stream(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    prep["module"].launch(args, 1, solver.block_size, 0, stream.cuda_stream)
+    e1.record(stream)
+    time.sleep(0.5)
+    flag[0] = 1
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    status = bufs["status"].cpu().numpy()
+    assert set(np.unique(status).tolist()) <= {0, 32}
+    assert np.sum(status == 32) > 0 and np.sum(status == 0) > 0
+    assert ms < 10_000.0, ms
