@@ -52,6 +52,9 @@ template <class T> __device__ __forceinline__ T absv(T v) { return v < T(0) ? -v
 // the forward bit for bit from different surroundings.
 __device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
 __device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+// Correctly rounded division (fast-math builds otherwise approximate it).
+__device__ __forceinline__ float div_rn(float a, float b) { return __fdiv_rn(a, b); }
+__device__ __forceinline__ double div_rn(double a, double b) { return __ddiv_rn(a, b); }
 
 // Type selection (A when B holds, else Bt) without the standard library,
 // which NVRTC does not provide.

@@ -116,8 +116,10 @@ struct Controller {
                 const G ratio = nrm2 * nrm2 / err_prev;
                 // the step-size ratio only scales a gain that is clamped to
                 // [min_gain, max_gain]: formed in the gain precision (an FP64
-                // division costs about as much as the rest of the update)
-                const G gain_gus = G(safety * (G(dt) / G(dt_prev)) * gpow(ratio, -expo));
+                // division costs about as much as the rest of the update),
+                // rounded correctly so that every build of the loop takes the
+                // same steps
+                const G gain_gus = G(safety * div_rn(G(dt), G(dt_prev)) * gpow(ratio, -expo));
                 gain = gain_gus < gain_basic ? gain_gus : gain_basic;
                 gain = (accept && dt_prev > C(1e-16)) ? gain : gain_basic;
                 st.hdt = commit_history ? current_dt : st.hdt;
