@@ -15,12 +15,20 @@ def test_hetero_launch_matches_separate_solves(cuda_device):
     solvers, batches = families()
     hs = HeteroSolver(solvers)
     results = hs.solve(batches, nan_error_trajectories=False)
+    # The heterogeneous module and a family's own module are separate
+    # compilations of the same loop: the compiler may fuse a multiply-add
+    # in one and not the other, and a stiff run's step sequence amplifies
+    # that last bit, so the bar is the FP32 parity bar (10 tolerance units)
+    # rather than bit identity (the CPU emulation of both, which fuses
+    # nothing, agrees bit for bit: test_hetero_emulated.py).
     for s, b, r in zip(solvers, batches, results):
         ref = s.solve(b["initial_values"], b["parameters"], duration=b["duration"], durations=b["durations"],
                       nan_error_trajectories=False)
         assert r.status_codes.tolist() == ref.status_codes.tolist()
-        np.testing.assert_array_equal(r.state, ref.state)
-        assert r.totals == ref.totals
+        atol, rtol = float(np.max(s.atol)), float(np.max(s.rtol))
+        err = np.abs(r.state.astype(np.float64) - ref.state) / (atol + rtol * np.abs(ref.state))
+        assert float(np.max(err)) < 10.0
+        assert abs(r.totals["steps"] - ref.totals["steps"]) <= 0.01 * ref.totals["steps"]
 
 
 def _vdp_solver(**kw):
@@ -126,8 +134,8 @@ def test_chunked_solve_equals_unchunked(cuda_device, tmp_path, per_run_horizons)
 def test_fp32_floor_routing_matches_separate_solves(cuda_device):
     """A mixed-precision family with per-run tolerances straddling the FP32
     floor: the runs below it come back from the FP64 twin family of the same
-    launch, bit-identical to an FP64 solve of those runs, the others
-    bit-identical to the mixed-precision solve, in the caller's order."""
+    launch and match an FP64 solve of those runs, the others match the
+    mixed-precision solve, in the caller's order."""
     from test_hetero_emulated import families
     from cubie_b200.hetero import FP32_RTOL_FLOOR, HeteroSolver
     solvers, batches = families()
@@ -143,4 +151,7 @@ def test_fp32_floor_routing_matches_separate_solves(cuda_device):
         ref = solver.solve(b["initial_values"][:, idx], b["parameters"][:, idx], duration=b["duration"],
                            durations=b["durations"][idx], tol_scale=ts[idx], nan_error_trajectories=False)
         assert r.status_codes[idx].tolist() == ref.status_codes.tolist()
-        np.testing.assert_array_equal(r.state[..., idx], ref.state.astype(np.float64))
+        # separate compilations: the FP32 parity bar (see the test above)
+        yr = ref.state.astype(np.float64)
+        err = np.abs(r.state[..., idx] - yr) / (1e-6 + 1e-6 * ts[idx] * np.abs(yr))
+        assert float(np.max(err)) < 10.0
