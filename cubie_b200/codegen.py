@@ -336,6 +336,16 @@ def generate_system(system: SymbolicODE, struct_name: str = "System", second_ord
         body = body if body.strip() else "        (void)0;"
         return f"    template <class R>\n    static __device__ __forceinline__ void {sig}\n    {{\n{body}\n    }}\n"
 
+    # M v for a constant mass matrix, row by row in column order, zero entries
+    # skipped (the reference's operator and residual generators,
+    # linear_operators.py:708-735, nonlinear_residuals.py:324-345)
+    mass_lines = []
+    if system.mass is not None:
+        for i in range(n):
+            terms = [("v[%d]" % j) if system.mass[i, j] == 1.0 else f"R({_lit_f(system.mass[i, j])})*v[{j}]"
+                     for j in range(n) if system.mass[i, j] != 0.0]
+            mass_lines.append(f"        out[{i}] = {' + '.join(terms) if terms else 'R(0)'};")
+
     unused = "(void)y; (void)p; (void)d; (void)t;"
     src = [f"struct {struct_name} {{",
            f"    static constexpr int N = {n};",
@@ -345,6 +355,9 @@ def generate_system(system: SymbolicODE, struct_name: str = "System", second_ord
            f"    static constexpr int NJ = {max(nnz, 1)};",
            f"    static constexpr bool HAS_DFDT = {str(any(e != 0 for e in dfdt)).lower()};",
            f"    static constexpr int NPJ = {max(len(pjac_pattern), 1)};",
+           f"    static constexpr bool HAS_MASS = {str(system.mass is not None).lower()};",
+           fn("mass_mv(const R* __restrict__ v, R* __restrict__ out)",
+              "        (void)v; (void)out;\n" + "\n".join(mass_lines)),
            fn("dxdt(const R* __restrict__ y, const R* __restrict__ p, const R* __restrict__ d, R t, R* __restrict__ f)",
               f"        {unused}\n" + body_f),
            fn("observables(const R* __restrict__ y, const R* __restrict__ p, const R* __restrict__ d, R t, R* __restrict__ o)",
@@ -370,6 +383,10 @@ def generate_system(system: SymbolicODE, struct_name: str = "System", second_ord
                            jac_pattern=jac_pattern, pjac_pattern=pjac_pattern, flops=flops)
 
 
+def _lit_f(x: float) -> str:
+    return repr(float(x))
+
+
 def system_stub(system: SymbolicODE, struct_name: str = "System") -> GeneratedSystem:
     """The size constants of ``system`` without any functions: the
     warp-per-system layout evaluates the system through its class-grouped
@@ -384,6 +401,7 @@ def system_stub(system: SymbolicODE, struct_name: str = "System") -> GeneratedSy
                      "    static constexpr int NJ = 1;",
                      "    static constexpr bool HAS_DFDT = true;",
                      "    static constexpr int NPJ = 1;",
+                     f"    static constexpr bool HAS_MASS = {str(system.mass is not None).lower()};",
                      "};"])
     return GeneratedSystem(name=system.name, source=src, n=n, n_params=system.num_parameters,
                            n_drivers=system.num_drivers, n_observables=system.num_observables,

@@ -43,11 +43,12 @@ __device__ __forceinline__ int linear_solve(const Op& op, typename Cfg::R* rhs, 
     }
 }
 
-// Single-stage operator A v = v - s J v with a Jacobian fixed for the solve
+// Single-stage operator A v = M v - s J v with a Jacobian fixed for the solve
 // (Rosenbrock: J at the step start and s = gamma h; DIRK Newton: J at
 // base + a_ii z and s = a_ii h).  Matches the generated operator
-// beta M v - gamma a_ij h J v with beta = 1 and M = I
-// (codegen/linear_operators.py:80-177) and the truncated Neumann
+// beta M v - gamma a_ij h J v with beta = 1, M the system's constant mass
+// matrix or the identity (codegen/linear_operators.py:80-177) and the
+// truncated Neumann
 // preconditioner out <- v + s J out repeated ``order`` times
 // (codegen/preconditioners.py:85-200).
 template <class Cfg>
@@ -63,8 +64,15 @@ struct SingleStageOp {
     __device__ __forceinline__ void apply(const R* v, R* out) const {
         R jv[K];
         Sys::template jmv<R>(J, v, jv);
+        if constexpr (Sys::HAS_MASS) {
+            R mv[K];
+            Sys::template mass_mv<R>(v, mv);
 #pragma unroll
-        for (int i = 0; i < K; ++i) out[i] = v[i] - s * jv[i];
+            for (int i = 0; i < K; ++i) out[i] = mv[i] - s * jv[i];
+        } else {
+#pragma unroll
+            for (int i = 0; i < K; ++i) out[i] = v[i] - s * jv[i];
+        }
     }
     __device__ __forceinline__ void precond(const R* v, R* out, R* scratch) const {
 #pragma unroll
@@ -116,8 +124,20 @@ struct CoupledOp {
     __device__ __forceinline__ void apply(const R* v, R* out) const {
         R jv[K];
         couple_jv(v, jv);
+        if constexpr (Sys::HAS_MASS) {
+            // M v_i - h J_i sum_j a_ij v_j per stage block
+            // (linear_operators.py:708-735)
 #pragma unroll
-        for (int i = 0; i < K; ++i) out[i] = v[i] - h * jv[i];
+            for (int i = 0; i < S; ++i) {
+                R mv[N];
+                Sys::template mass_mv<R>(v + i * N, mv);
+#pragma unroll
+                for (int k = 0; k < N; ++k) out[i * N + k] = mv[k] - h * jv[i * N + k];
+            }
+        } else {
+#pragma unroll
+            for (int i = 0; i < K; ++i) out[i] = v[i] - h * jv[i];
+        }
     }
     __device__ __forceinline__ void precond(const R* v, R* out, R* scratch) const {
 #pragma unroll

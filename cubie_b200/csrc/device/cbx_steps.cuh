@@ -367,6 +367,13 @@ struct FirkProblem {
             Sys::template dxdt<R>(Y, ctx->p, drv[i], t + h * R(Tab::c(i)), f);
 #pragma unroll
             for (int k = 0; k < N; ++k) out[i * N + k] = u[i * N + k] - h * f[k];
+            if constexpr (Sys::HAS_MASS) {
+                // M u_i - h f(Y_i) (nonlinear_residuals.py:324-345)
+                R mu[N];
+                Sys::template mass_mv<R>(u + i * N, mu);
+#pragma unroll
+                for (int k = 0; k < N; ++k) out[i * N + k] = mu[k] - h * f[k];
+            }
         }
     }
     __device__ __forceinline__ void linearize(const R* u) {
@@ -550,8 +557,16 @@ struct DirkProblem {
 #pragma unroll
         for (int k = 0; k < N; ++k) Y[k] = base[k] + a * z[k];
         Sys::template dxdt<R>(Y, ctx->p, drv, t, f);
+        if constexpr (Sys::HAS_MASS) {
+            // M z - h f(base + a z) (nonlinear_residuals.py:59-130)
+            R mz[N];
+            Sys::template mass_mv<R>(z, mz);
 #pragma unroll
-        for (int k = 0; k < N; ++k) out[k] = z[k] - h * f[k];
+            for (int k = 0; k < N; ++k) out[k] = mz[k] - h * f[k];
+        } else {
+#pragma unroll
+            for (int k = 0; k < N; ++k) out[k] = z[k] - h * f[k];
+        }
     }
     __device__ __forceinline__ void linearize(const R* z) {
         R Y[N];

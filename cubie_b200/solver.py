@@ -146,6 +146,16 @@ class Solver:
         if layout not in ("thread", "warp"):
             raise ValueError("layout must be 'thread', 'warp' or 'auto'")
         self.layout = layout
+        if getattr(system, "mass", None) is not None:
+            # SingleIntegratorRunCore.py:765-780
+            if self.tableau.kind == "erk":
+                raise ValueError("The system defines a mass matrix and requires an implicit algorithm; "
+                                 f"'{self.algorithm}' does not consume a mass matrix and would integrate the "
+                                 "constraint residuals as derivatives.")
+            if layout == "warp":
+                raise NotImplementedError("the warp-per-system layout takes systems without a mass matrix")
+            if execution.get("adjoint"):
+                raise NotImplementedError("the discrete adjoint takes systems without a mass matrix")
         # warp layout: stage-solve scratch vectors in "shared" memory or
         # "local" (registers / local memory; the faster of the two on the
         # 256-state cable); "auto" lets the autotuner pick

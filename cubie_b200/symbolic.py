@@ -179,7 +179,7 @@ class SymbolicODE:
                  observables: List[str], assignments: List[Tuple[sp.Symbol, sp.Expr]],
                  derivatives: Dict[str, sp.Expr], precision=np.float32,
                  name: Optional[str] = None, driver_settings: Optional[dict] = None,
-                 source: str = ""):
+                 source: str = "", mass=None):
         self.state_names = list(states)
         self.initial_values = dict(states)
         self.parameter_names = list(parameters)
@@ -192,6 +192,19 @@ class SymbolicODE:
         self.derivatives = derivatives
         self.precision = np.dtype(precision).type
         self.driver_settings = driver_settings
+        # constant mass matrix M of M y' = f(t, y) (None: identity), paired
+        # row for row with the state order (symbolicODE.py ``mass``)
+        n = len(self.state_names)
+        if mass is not None:
+            m = np.asarray(mass, dtype=np.float64)
+            if m.shape != (n, n):
+                raise ValueError(f"mass matrix has shape {m.shape}; expected ({n}, {n})")
+            if not np.all(np.isfinite(m)):
+                raise ValueError("mass matrix entries must be finite")
+            mass = None if np.array_equal(m, np.eye(n)) else m
+        self.mass = mass
+        if mass is not None:
+            source = source + "|M" + ",".join(repr(float(v)) for v in mass.ravel())
         self._source = source
         self.fn_hash = hashlib.sha256(
             (source + repr(sorted(self.constants.items())) + str(np.dtype(self.precision))).encode()
@@ -209,7 +222,8 @@ class SymbolicODE:
         return SymbolicODE(states=self.initial_values, parameters=self.parameters, constants=self.constants,
                            drivers=self.driver_names, observables=self.observable_names,
                            assignments=self.assignments, derivatives=self.derivatives, precision=precision,
-                           name=self.name, driver_settings=self.driver_settings, source=self._source)
+                           name=self.name, driver_settings=self.driver_settings,
+                           source=self._source.split("|M")[0], mass=self.mass)
 
     # -- sizes ---------------------------------------------------------
     @property
@@ -302,6 +316,7 @@ def create_ODE_system(
     drivers: Optional[Union[Iterable[str], Mapping[str, object]]] = None,
     name: Optional[str] = None,
     strict: bool = False,
+    mass=None,
     **unsupported,
 ) -> SymbolicODE:
     """Build a :class:`SymbolicODE` from ``lhs = rhs`` equation strings.
@@ -312,6 +327,10 @@ def create_ODE_system(
     ``dX`` left-hand sides and undeclared right-hand-side names become
     parameters (default 0), as the reference's inference does
     (``parsing/parser.py:715-800``); ``strict=True`` raises instead.
+    ``mass`` is a constant mass matrix M (``M y' = f``, states in declared
+    order; ``None`` is the identity), as the reference's ``mass`` argument:
+    a singular M makes a semi-explicit DAE and needs an implicit
+    algorithm.
     """
     for key, value in unsupported.items():
         if value not in (None, False, {}):
@@ -403,7 +422,7 @@ def create_ODE_system(
                        constants=const_defaults, drivers=driver_names,
                        observables=obs_names, assignments=assignments,
                        derivatives=derivatives, precision=precision, name=name,
-                       driver_settings=driver_settings, source=source)
+                       driver_settings=driver_settings, source=source, mass=mass)
 
 
 def _topological(assignments, base_names):

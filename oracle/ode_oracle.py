@@ -16,6 +16,10 @@ Followed files (reference, ``src/cubie/``):
   Rosenbrock step  integrators/algorithms/generic_rosenbrock_w.py:459-759
   FIRK step        integrators/algorithms/generic_firk.py:508-701
   DIRK step        integrators/algorithms/generic_dirk.py:515-855
+  mass matrix      odesystems/symbolic/codegen/linear_operators.py:708-735,
+                   nonlinear_residuals.py:59-130,324-345 (M v and M u terms;
+                   Rosenbrock's C_ij k_j / h term without M, as the
+                   reference forms it: generic_rosenbrock_w.py:682-698)
   dense predictor  integrators/stage_predictors.py:76-548
   Newton           integrators/matrix_free_solvers/newton_krylov.py:340-517
   MR / SD          integrators/matrix_free_solvers/linear_solver.py:220-385
@@ -239,8 +243,11 @@ class OracleSystem:
 
     def __init__(self, equations: Sequence[str], states: Sequence[str], parameters: Sequence[str] = (),
                  constants: Optional[Dict[str, float]] = None, observables: Sequence[str] = (),
-                 drivers: Sequence[str] = ()):
+                 drivers: Sequence[str] = (), mass=None):
         constants = constants or {}
+        # constant mass matrix of M y' = f (None: identity), as the
+        # reference's create_ODE_system ``mass`` (symbolicODE.py:179-184)
+        self.mass = None if mass is None else np.asarray(mass, dtype=np.float64)
         self.states = list(states)
         self.parameters = list(parameters)
         self.observables = list(observables)
@@ -277,6 +284,12 @@ class OracleSystem:
         dfdt = [sp.diff(e, t) + sum((sp.diff(e, d) * dd for d, dd in zip(ds, dds)), sp.Integer(0)) for e in f]
         self._dt = sp.lambdify((t, ys, ps, ds, dds), dfdt, "numpy")
         self._obs = sp.lambdify(args, [table[o] for o in self.observables], "numpy") if self.observables else None
+
+    def mv(self, v: np.ndarray) -> np.ndarray:
+        """M v for every run (rows of ``v``); v itself without a mass matrix."""
+        if self.mass is None:
+            return v
+        return (v @ self.mass.T.astype(v.dtype)).astype(v.dtype)
 
     def _drv(self, t, B, dtype, derivative=False):
         """Driver values (or time derivatives) at ``t`` for every run."""
@@ -552,6 +565,8 @@ def integrate(system: OracleSystem, algorithm: str, inits: np.ndarray, params: n
     mixed = ct != rt
     tab = TABLEAUS[algorithm]
     n = system.n
+    if getattr(system, "mass", None) is not None and tab.kind == "erk":
+        raise ValueError("a mass matrix needs an implicit algorithm")
     B = inits.shape[1]
     Y = np.ascontiguousarray(inits.T.astype(rt))
     P = np.ascontiguousarray(params.T.astype(rt)) if params.size else np.zeros((B, 0), rt)
@@ -923,7 +938,7 @@ def integrate(system: OracleSystem, algorithm: str, inits: np.ndarray, params: n
     def single_op(J, s_coef, ref):
         """A v = v - s J v and its Neumann preconditioner (order m)."""
         def A(v):
-            return v - s_coef[:, None] * np.einsum("bij,bj->bi", J, v)
+            return system.mv(v) - s_coef[:, None] * np.einsum("bij,bj->bi", J, v)
 
         def Pc(v):
             out = v.copy()
@@ -1104,7 +1119,7 @@ def integrate(system: OracleSystem, algorithm: str, inits: np.ndarray, params: n
                 out = np.zeros_like(u)
                 for i, Ys in enumerate(stage_states_of(u)):
                     fi = system.f(tt + h * rt(tab.c[i]), Ys, P)
-                    out[:, i * n:(i + 1) * n] = u[:, i * n:(i + 1) * n] - h[:, None] * fi
+                    out[:, i * n:(i + 1) * n] = system.mv(u[:, i * n:(i + 1) * n]) - h[:, None] * fi
                 return out
 
             def op_builder(u):
@@ -1121,7 +1136,8 @@ def integrate(system: OracleSystem, algorithm: str, inits: np.ndarray, params: n
                     return out
 
                 def A(v):
-                    return v - h[:, None] * cjv(v)
+                    mv = np.concatenate([system.mv(v[:, i * n:(i + 1) * n]) for i in range(s)], axis=1)
+                    return mv - h[:, None] * cjv(v)
 
                 def Pc(v):
                     out = v.copy()
@@ -1213,7 +1229,7 @@ def integrate(system: OracleSystem, algorithm: str, inits: np.ndarray, params: n
                     bb = base.copy()
 
                     def res_fn(zz, bb=bb, a_c=a_c, st_time=st_time):
-                        return zz - h[:, None] * system.f(st_time, bb + a_c * zz, P)
+                        return system.mv(zz) - h[:, None] * system.f(st_time, bb + a_c * zz, P)
 
                     def op_builder(zz, bb=bb, a_c=a_c, st_time=st_time):
                         J = system.jac(st_time, bb + a_c * zz, P)

@@ -80,6 +80,26 @@ def vdp_manifold_inputs(x0s, mus):
     return x0, np.asarray(mus, dtype=float)[None, :]
 
 
+# Constant mass matrices (the reference's ``mass`` argument of
+# create_ODE_system): a semi-explicit index-1 DAE (Robertson kinetics with
+# its conservation law as the algebraic row, M = diag(1, 1, 0)) and Van der
+# Pol with a full, nonsingular M.
+ROBER_DAE = dict(
+    equations=["dy1 = -k1 * y1 + k3 * y2 * y3", "dy2 = k1 * y1 - k3 * y2 * y3 - k2 * y2**2",
+               "dy3 = y1 + y2 + y3 - 1"],
+    states=["y1", "y2", "y3"], parameters=["k1", "k2", "k3"], constants={},
+    mass=[[1.0, 0.0, 0.0], [0.0, 1.0, 0.0], [0.0, 0.0, 0.0]],
+)
+VDP_MASS = dict(VDP, mass=[[2.0, 0.5], [0.5, 1.0]])
+
+
+def rober_inputs(n, seed):
+    rng = np.random.default_rng(seed)
+    x0 = np.tile(np.array([[1.0], [0.0], [0.0]]), (1, n))
+    p = np.stack([0.04 * rng.uniform(0.5, 2, n), 3e7 * rng.uniform(0.5, 2, n), 1e4 * rng.uniform(0.5, 2, n)])
+    return x0, p
+
+
 def lorenz_inputs(n, seed):
     rng = np.random.default_rng(seed)
     rho = rng.uniform(20.0, 35.0, n)
@@ -304,6 +324,25 @@ CASES.update({
 })
 
 
+CASES.update({
+    "rober_dae_radau_f64": dict(system=ROBER_DAE, algorithm="radau", precision="float64", inputs=("rober", 3, 70),
+                                duration=1.0, kwargs=dict(rtol=1e-6, atol=1e-8, save_every=0.25, output_types=_ITS)),
+    "rober_dae_dirk3_f64": dict(system=ROBER_DAE, algorithm="l_stable_dirk_3", precision="float64",
+                                inputs=("rober", 3, 71), duration=0.5,
+                                kwargs=dict(dt=1e-3, rtol=1e-6, atol=1e-8, save_every=0.125,
+                                            linear_correction_type="bicgstab", output_types=_ITS)),
+    "rober_dae_ros3p_f64": dict(system=ROBER_DAE, algorithm="ros3p", precision="float64", inputs=("rober", 3, 72),
+                                duration=1.0, kwargs=dict(rtol=1e-6, atol=1e-8, save_every=0.25,
+                                                          linear_correction_type="bicgstab", output_types=_ITS)),
+    "vdp_mass_ros3p_f64": dict(system=VDP_MASS, algorithm="ros3p", precision="float64",
+                               inputs=("vdp", 3, 73, [1.0, 3.0, 10.0]), duration=2.0,
+                               kwargs=dict(rtol=1e-7, atol=1e-7, save_every=0.5, output_types=_ITS)),
+    "vdp_mass_radau_f32": dict(system=VDP_MASS, algorithm="radau", precision="float32",
+                               inputs=("vdp", 3, 74, [1.0, 3.0, 10.0]), duration=2.0,
+                               kwargs=dict(rtol=1e-6, atol=1e-6, save_every=0.5, output_types=_ITS)),
+})
+
+
 def case_inputs(case):
     kind = case["inputs"][0]
     if kind == "lorenz":
@@ -316,6 +355,8 @@ def case_inputs(case):
         return driven_inputs(case["inputs"][1], case["inputs"][2])
     if kind == "hh":
         return hh_inputs(case["inputs"][1], case["inputs"][2])
+    if kind == "rober":
+        return rober_inputs(case["inputs"][1], case["inputs"][2])
     if kind == "vdp_manifold":
         return vdp_manifold_inputs(case["inputs"][1], case["inputs"][2])
     raise KeyError(kind)

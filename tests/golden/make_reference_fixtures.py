@@ -40,7 +40,8 @@ prec = np.dtype(case["precision"]).type
 drivers = case_drivers(case)
 system = create_ODE_system(dxdt=sysd["equations"], states={{s: 0.0 for s in sysd["states"]}},
                            parameters={{p: 0.0 for p in sysd["parameters"]}}, constants=sysd["constants"],
-                           drivers=sysd.get("drivers"), precision=prec, name="fixture_" + name, strict=True)
+                           drivers=sysd.get("drivers"), precision=prec, name="fixture_" + name, strict=True,
+                           **({{"mass": np.asarray(sysd["mass"], dtype=prec)}} if sysd.get("mass") is not None else {{}}))
 inits, params = case_inputs(case)
 solver = Solver(system, algorithm=case["algorithm"], cache=False, auto_memory=False, **case["kwargs"])
 t = time.time()

@@ -15,7 +15,7 @@ def build_case_system(case):
     prec = np.dtype(case["precision"]).type
     return create_ODE_system(sd["equations"], states={s: 0.0 for s in sd["states"]},
                              parameters={p: 0.0 for p in sd["parameters"]}, constants=sd["constants"],
-                             drivers=sd.get("drivers"), precision=prec, strict=True)
+                             drivers=sd.get("drivers"), precision=prec, strict=True, mass=sd.get("mass"))
 
 
 def oracle_driver_table(case, name):
@@ -32,7 +32,7 @@ def run_oracle(case, **overrides):
     from oracle import OracleSystem, integrate
     sd = case["system"]
     osys = OracleSystem(sd["equations"], sd["states"], sd["parameters"], sd["constants"],
-                        drivers=sd.get("drivers", ()))
+                        drivers=sd.get("drivers", ()), mass=sd.get("mass"))
     if sd.get("drivers"):
         name = next(n for n, c in CASES.items() if c is case)
         osys.driver_table = oracle_driver_table(case, name)
