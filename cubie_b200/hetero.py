@@ -24,6 +24,7 @@ import numpy as np
 from . import _native
 from .kernelgen import generate_hetero_kernel
 from .solver import Solver, _is_tensor, _torch
+from .solveresult import merge_results
 
 _HETERO_MODULES: Dict[tuple, "_native.Module"] = {}
 
@@ -182,9 +183,30 @@ class HeteroSolver:
         return launch
 
     def solve(self, batches: Sequence[Dict[str, Any]], nan_error_trajectories: bool = True,
-              on_device: bool = False, stream=None) -> List:
+              on_device: bool = False, stream=None, distributed: bool = False) -> List:
         """Integrate every family's batch with one launch; one SolveResult
-        per family."""
+        per family.  ``distributed=True`` splits every family's runs across
+        the ranks of the initialised ``torch.distributed`` group
+        (interleaved, so each rank's launch holds the same mix of families
+        and horizons); every rank returns the whole batch's results."""
+        import torch.distributed as dist
+        if distributed and dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1:
+            from .shard import interleaved_runs
+            rank, world = dist.get_rank(), dist.get_world_size()
+            sizes = [int(b["initial_values"].shape[-1]) for b in batches]
+            local = []
+            for b, n in zip(batches, sizes):
+                idx = interleaved_runs(n, rank, world)
+                sub = dict(b)
+                for key in ("initial_values", "parameters", "durations", "tol_scale"):
+                    if b.get(key) is not None:
+                        sub[key] = _take(b[key], idx)
+                local.append(sub)
+            mine = self.solve(local, nan_error_trajectories, False, stream)
+            parts = [None] * world
+            dist.all_gather_object(parts, mine)
+            return [merge_results([(parts[r][k], interleaved_runs(n, r, world)) for r in range(world)])
+                    for k, n in enumerate(sizes)]
         run = self.setup(batches)
         self.last_kernel_ms = run.timed_launch(stream)
         return run.collect(nan_error_trajectories, on_device)
@@ -252,30 +274,3 @@ class HeteroLaunch:
                     raise ValueError("routed families are merged on the host (on_device=False)")
                 out.append(merge_results([(per_launch[f], idx) for f, idx in route]))
         return out
-
-
-def merge_results(parts) -> "SolveResult":
-    """Reassemble one family's SolveResult from sub-results over disjoint run
-    index sets ``[(result, run_indices), ...]`` (arrays promoted to the
-    widest dtype among the parts; totals summed)."""
-    import copy
-    first = parts[0][0]
-    n = sum(len(idx) for _, idx in parts)
-    res = copy.copy(first)
-    for name in ("state", "observables", "state_summaries", "observable_summaries", "iteration_counters"):
-        arrs = [getattr(r, name) for r, _ in parts]
-        if any(a is None for a in arrs):
-            setattr(res, name, None)
-            continue
-        dtype = np.result_type(*arrs)
-        full = np.empty(arrs[0].shape[:-1] + (n,), dtype=dtype)
-        for a, (_, idx) in zip(arrs, parts):
-            full[..., idx] = a
-        setattr(res, name, full)
-    status = np.empty(n, dtype=first.status_codes.dtype)
-    for r, idx in parts:
-        status[idx] = r.status_codes
-    res.status_codes = status
-    if all(r.totals is not None for r, _ in parts):
-        res.totals = {k: sum(r.totals[k] for r, _ in parts) for k in first.totals}
-    return res

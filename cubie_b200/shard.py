@@ -10,7 +10,7 @@ per-rank counts, so that a whole-job rate is total work / slowest rank.
 
 from __future__ import annotations
 
-from typing import Optional, Sequence, Tuple
+from typing import Callable, Dict, Optional, Sequence, Tuple
 
 import numpy as np
 
@@ -52,3 +52,45 @@ def aggregate(ms: float, count: float, group=None, device=None) -> Tuple[float, 
     dist.all_reduce(tm, op=dist.ReduceOp.MAX, group=group)
     dist.all_reduce(ts, op=dist.ReduceOp.SUM, group=group)
     return float(tm[0]), float(ts[0])
+
+
+def interleaved_runs(n_total: int, rank: int, world: int) -> np.ndarray:
+    """Run indices ``rank, rank + world, ...`` of a strided split: every
+    rank gets the same mix of short and long runs (and, for a batch that
+    concatenates several systems, of every system)."""
+    if world < 1 or not 0 <= rank < world:
+        raise ValueError("rank must be in [0, world)")
+    return np.arange(rank, int(n_total), world, dtype=np.int64)
+
+
+def _take_runs(x, idx):
+    if x is None:
+        return None
+    if hasattr(x, "index_select") and hasattr(x, "device"):
+        import torch
+        return x.index_select(x.dim() - 1, torch.as_tensor(idx, device=x.device, dtype=torch.long))
+    return np.asarray(x)[..., idx]
+
+
+def distributed_solve(solve: Callable, initial_values, parameters, per_run: Optional[Dict] = None,
+                      group=None):
+    """Integrate a batch across the ranks of a ``torch.distributed`` group,
+    one process per GPU: each rank integrates its interleaved share of the
+    runs with ``solve(inits, params, **per_run_share)`` (a SolveResult), and
+    every rank returns the whole batch's SolveResult in the caller's run
+    order.  The integration exchanges nothing; the results are gathered
+    once at the end (``all_gather_object``: over NCCL or gloo).  Without an
+    initialised group (or with one rank) it is ``solve`` itself."""
+    import torch.distributed as dist
+    per_run = dict(per_run or {})
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size(group) == 1:
+        return solve(initial_values, parameters, **per_run)
+    from .solveresult import merge_results
+    rank, world = dist.get_rank(group), dist.get_world_size(group)
+    n = int(initial_values.shape[-1])
+    idx = interleaved_runs(n, rank, world)
+    share = {k: _take_runs(v, idx) for k, v in per_run.items()}
+    local = solve(_take_runs(initial_values, idx), _take_runs(parameters, idx), **share)
+    parts = [None] * world
+    dist.all_gather_object(parts, local, group=group)
+    return merge_results([(r, interleaved_runs(n, k, world)) for k, r in enumerate(parts)])

@@ -534,9 +534,29 @@ class Solver:
               settling_time: float = 0.0, t0: float = 0.0, blocksize: Optional[int] = None,
               grid_type: str = "verbatim", nan_error_trajectories: bool = True,
               on_device: bool = False, durations=None, tol_scale=None, stream=None,
-              **kwargs) -> SolveResult:
+              distributed: bool = False, **kwargs) -> SolveResult:
+        """``distributed=True`` splits the runs across the ranks of the
+        initialised ``torch.distributed`` group (one process per GPU, each
+        solver on its own device): every rank integrates an interleaved
+        share and returns the whole batch's result (no exchange during the
+        integration; the outputs are gathered once at the end)."""
         if kwargs:
             raise KeyError(f"Unrecognized keyword arguments: {set(kwargs)}")
+        if distributed:
+            if on_device:
+                raise ValueError("a distributed solve returns host arrays (on_device=False)")
+            from .shard import distributed_solve
+            if not (_is_tensor(initial_values) and _is_tensor(parameters)):
+                initial_values, parameters = self.build_grid(initial_values, parameters, grid_type)
+
+            def local(iv, pv, durations=None, tol_scale=None):
+                return self.solve(iv, pv, drivers=drivers, duration=duration, settling_time=settling_time, t0=t0,
+                                  blocksize=blocksize, nan_error_trajectories=nan_error_trajectories,
+                                  durations=durations, tol_scale=tol_scale, stream=stream)
+
+            return distributed_solve(local, initial_values, parameters,
+                                     {k: v for k, v in (("durations", durations), ("tol_scale", tol_scale))
+                                      if v is not None})
         if drivers is not None or self.system.num_drivers > 0:
             from .interpolator import ArrayInterpolator
             interp = ArrayInterpolator.from_system(self.system, drivers, self.precision)

@@ -135,3 +135,30 @@ class SolveResult:
                 frames.append(df)
             out["summaries"] = pd.concat(frames, ignore_index=True)
         return out
+
+
+def merge_results(parts) -> SolveResult:
+    """Reassemble one family's SolveResult from sub-results over disjoint run
+    index sets ``[(result, run_indices), ...]`` (arrays promoted to the
+    widest dtype among the parts; totals summed)."""
+    import copy
+    first = parts[0][0]
+    n = sum(len(idx) for _, idx in parts)
+    res = copy.copy(first)
+    for name in ("state", "observables", "state_summaries", "observable_summaries", "iteration_counters"):
+        arrs = [getattr(r, name) for r, _ in parts]
+        if any(a is None for a in arrs):
+            setattr(res, name, None)
+            continue
+        dtype = np.result_type(*arrs)
+        full = np.empty(arrs[0].shape[:-1] + (n,), dtype=dtype)
+        for a, (_, idx) in zip(arrs, parts):
+            full[..., idx] = a
+        setattr(res, name, full)
+    status = np.empty(n, dtype=first.status_codes.dtype)
+    for r, idx in parts:
+        status[idx] = r.status_codes
+    res.status_codes = status
+    if all(r.totals is not None for r, _ in parts):
+        res.totals = {k: sum(r.totals[k] for r, _ in parts) for k in first.totals}
+    return res
