@@ -33,7 +33,7 @@ GOLDEN = Path(__file__).resolve().parent / "golden"
 # expression order differs from the reference's printer in these systems
 ROUNDING_ONLY = {"fhn_dp54_peaks_f32": 10.0, "fhn_dp54_derivs_f32": 10.0, "fhn_dp54_derivs_f64": 1e-3,
                  "driven_dp54_clamped_f64": 1e-3, "driven_ros3p_clamped_f64": 1e-3,
-                 "hh64_dirk3_bicgstab_f32": 10.0}
+                 "hh64_dirk3_bicgstab_f32": 10.0, "rober_dae_dirk3_f64": 1e-3, "rober_dae_radau_f64": 1e-3}
 
 
 @pytest.mark.parametrize("name", list(CASES))
