@@ -52,9 +52,6 @@ template <class T> __device__ __forceinline__ T absv(T v) { return v < T(0) ? -v
 // the forward bit for bit from different surroundings.
 __device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
 __device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
-// Correctly rounded division (fast-math builds otherwise approximate it).
-__device__ __forceinline__ float div_rn(float a, float b) { return __fdiv_rn(a, b); }
-__device__ __forceinline__ double div_rn(double a, double b) { return __ddiv_rn(a, b); }
 
 // Type selection (A when B holds, else Bt) without the standard library,
 // which NVRTC does not provide.
@@ -70,6 +67,10 @@ __device__ __forceinline__ float sqrt_t(float v) { return sqrtf(v); }
 __device__ __forceinline__ double sqrt_t(double v) { return sqrt(v); }
 __device__ __forceinline__ float pow_t(float a, float b) { return powf(a, b); }
 __device__ __forceinline__ double pow_t(double a, double b) { return pow(a, b); }
+__device__ __forceinline__ float log2_t(float a) { return log2f(a); }
+__device__ __forceinline__ double log2_t(double a) { return log2(a); }
+__device__ __forceinline__ float exp2_t(float a) { return exp2f(a); }
+__device__ __forceinline__ double exp2_t(double a) { return exp2(a); }
 
 template <class T> struct Limits;
 template <> struct Limits<float> {

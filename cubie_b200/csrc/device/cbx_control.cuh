@@ -35,9 +35,13 @@ struct Controller {
         G h0, h1;   // previous error norms (PI, PID); h1: previous norm (Gustafsson)
         C hdt;      // previous accepted step size (Gustafsson)
     };
+    // On the mixed-precision path Gustafsson's previous norm is kept as
+    // log2(max(norm, 1e-16)): both of its powers then come from one log2 of
+    // the current norm (no reference counterpart, so no bit pattern to keep).
+    static constexpr bool LOG_GUS = Cfg::MIXED && Cfg::CTRL == CTRL_GUSTAFSSON;
     static __device__ __forceinline__ void init(State& st) {
         st.h0 = G(0);
-        st.h1 = G(0);
+        st.h1 = LOG_GUS ? G(-53.150849518197795) : G(0);   // log2(1e-16)
         st.hdt = C(0);
     }
     static __device__ __forceinline__ G gpow(G a, G b) { return pow_t(a, b); }
@@ -107,23 +111,31 @@ struct Controller {
             } else {  // Gustafsson (gustafsson_controller.py:236-283)
                 const G expo = G(Cfg::CTL_E1);
                 const C dt_prev = pymax(st.hdt, C(1e-16));
-                const G err_prev = pymax(st.h1, G(1e-16));
                 const G gain_numerator = G(1 + 2 * Cfg::CTL_NEWTON_TARGET) * safety;
                 const G denom = G(niters + 2 * Cfg::CTL_NEWTON_TARGET);
                 const G tmp = gain_numerator / denom;
                 const G fac = safety < tmp ? safety : tmp;
-                const G gain_basic = G(fac * gpow(nrm2, -expo));
-                const G ratio = nrm2 * nrm2 / err_prev;
-                // the step-size ratio only scales a gain that is clamped to
-                // [min_gain, max_gain]: formed in the gain precision (an FP64
-                // division costs about as much as the rest of the update),
-                // rounded correctly so that every build of the loop takes the
-                // same steps
-                const G gain_gus = G(safety * div_rn(G(dt), G(dt_prev)) * gpow(ratio, -expo));
-                gain = gain_gus < gain_basic ? gain_gus : gain_basic;
-                gain = (accept && dt_prev > C(1e-16)) ? gain : gain_basic;
+                if constexpr (LOG_GUS) {
+                    // nrm2^-e and (nrm2^2 / prev)^-e from one log2; the step
+                    // ratio in the gain precision (an FP64 division costs
+                    // about as much as the rest of the update)
+                    const G l2 = log2_t(nrm2);
+                    const G lprev = pymax(st.h1, G(-53.150849518197795));
+                    const G gain_basic = fac * exp2_t(-expo * l2);
+                    const G gain_gus = safety * (G(dt) / G(dt_prev)) * exp2_t(-expo * (G(2) * l2 - lprev));
+                    gain = gain_gus < gain_basic ? gain_gus : gain_basic;
+                    gain = (accept && dt_prev > C(1e-16)) ? gain : gain_basic;
+                    st.h1 = commit_history ? l2 : st.h1;
+                } else {
+                    const G err_prev = pymax(st.h1, G(1e-16));
+                    const G gain_basic = G(fac * gpow(nrm2, -expo));
+                    const G ratio = nrm2 * nrm2 / err_prev;
+                    const G gain_gus = G(safety * G(dt / dt_prev) * gpow(ratio, -expo));
+                    gain = gain_gus < gain_basic ? gain_gus : gain_basic;
+                    gain = (accept && dt_prev > C(1e-16)) ? gain : gain_basic;
+                    st.h1 = commit_history ? nrm2 : st.h1;
+                }
                 st.hdt = commit_history ? current_dt : st.hdt;
-                st.h1 = commit_history ? nrm2 : st.h1;
             }
             gain = finish_gain(gain, accept);
             const bool freeze = accept && truncated;

@@ -287,7 +287,9 @@ __device__ __forceinline__ bool lane_iterate(Lane<Cfg>& L, const cbx_solve_args 
     Iters its;
     const int step_status = Step::step(ctx, L.y, ynew, delta, err, L.drv, drv_new, R(dt_eff), R(L.tp),
                                        L.first_step, L.prev_accepted, L.ps, its);
-    const int nit = its.nit, kit = its.kit;
+    // Rosenbrock steps report no Newton iterations: a constant here lets the
+    // controller's iteration-dependent factor fold away
+    const int nit = Cfg::ALGO == ALGO_ROSENBROCK ? 0 : its.nit, kit = its.kit;
     L.first_step = false;
     L.iteration_status |= step_status;
     const bool step_failed = step_status != SUCCESS;

@@ -34,6 +34,12 @@ _HETERO_MODULES: Dict[tuple, "_native.Module"] = {}
 # operation, and the reference's own gate rejects FP32 results below about
 # 1e-6 (tests/integrated_numerical_tests/julia_reference/ne_gate.py:38-41).
 FP32_RTOL_FLOOR = 1e-6
+# The same for the mixed-precision path (FP32 stages, FP64 time and control,
+# compensated state update): its state accumulates increments at FP64-like
+# accuracy, and on the mixed three-system batch its runs at rtol down to
+# 1e-8 match the error of the same method stepped in FP64; the floor sits a
+# decade below that.
+MIXED_RTOL_FLOOR = 1e-9
 
 
 def _take(x, idx):
@@ -49,15 +55,15 @@ def _take(x, idx):
 class HeteroSolver:
     """One launch over the runs of several solvers.
 
-    ``fp32_floor``: runs of an FP32 (or mixed-precision) family whose
-    tightest relative tolerance (``rtol`` x the run's ``tol_scale``) lies
-    below it are integrated by an FP64-stepping twin of that family, added
-    to the same launch; the family's results come back merged in the
-    caller's run order (in FP64 when any run was routed).  ``None`` turns
-    the routing off."""
+    ``fp32_floor`` / ``mixed_floor``: runs of an FP32 (or a
+    mixed-precision) family whose tightest relative tolerance (``rtol`` x
+    the run's ``tol_scale``) lies below it are integrated by an
+    FP64-stepping twin of that family, added to the same launch; the
+    family's results come back merged in the caller's run order (in FP64
+    when any run was routed).  ``None`` turns the routing off."""
 
     def __init__(self, solvers: Sequence[Solver], block_size: Optional[int] = None,
-                 fp32_floor: Optional[float] = FP32_RTOL_FLOOR):
+                 fp32_floor: Optional[float] = FP32_RTOL_FLOOR, mixed_floor: Optional[float] = MIXED_RTOL_FLOOR):
         if not 1 <= len(solvers) <= _native.HeteroArgs.MAX_FAMILIES:
             raise ValueError(f"one to {_native.HeteroArgs.MAX_FAMILIES} solvers per launch")
         devices = {s.device for s in solvers}
@@ -68,6 +74,7 @@ class HeteroSolver:
         self.device = devices.pop()
         self.block_size = int(block_size or solvers[0].block_size)
         self.fp32_floor = fp32_floor
+        self.mixed_floor = mixed_floor
         self.last_kernel_ms = None
         self._twins: Dict[int, Solver] = {}
 
@@ -80,11 +87,12 @@ class HeteroSolver:
             iv = b["initial_values"]
             n = int(iv.shape[1]) if hasattr(iv, "shape") and len(iv.shape) == 2 else None
             low = None
-            if self.fp32_floor is not None and s.precision == np.float32 and n is not None:
+            floor = self.mixed_floor if s.mixed_precision else self.fp32_floor
+            if floor is not None and s.precision == np.float32 and n is not None:
                 ts = b.get("tol_scale")
                 scale = np.ones(n) if ts is None else np.asarray(
                     ts.detach().cpu().numpy() if _is_tensor(ts) else ts, dtype=np.float64).reshape(-1)
-                low = float(np.min(s.rtol)) * scale < self.fp32_floor
+                low = float(np.min(s.rtol)) * scale < floor
             if low is None or not low.any():
                 routes.append([(len(fams), None)])
                 fams.append((s, b))

@@ -63,7 +63,5 @@ inline int __popc(unsigned v) { return __builtin_popcount(v); }
 // the host build contracts nothing, so they are plain adds here
 inline float __fadd_rn(float a, float b) { return a + b; }
 inline double __dadd_rn(double a, double b) { return a + b; }
-inline float __fdiv_rn(float a, float b) { return a / b; }
-inline double __ddiv_rn(double a, double b) { return a / b; }
 template <class T> inline T __shfl_sync(unsigned, T v, int) { return v; }
 inline bool __any_sync(unsigned, bool v) { return v; }

@@ -132,13 +132,13 @@ def test_chunked_solve_equals_unchunked(cuda_device, tmp_path, per_run_horizons)
 
 
 def test_fp32_floor_routing_matches_separate_solves(cuda_device):
-    """A mixed-precision family with per-run tolerances straddling the FP32
-    floor: the runs below it come back from the FP64 twin family of the same
-    launch and match an FP64 solve of those runs, the others match the
-    mixed-precision solve, in the caller's order."""
-    from test_hetero_emulated import families
+    """An FP32 family with per-run tolerances straddling the FP32 floor (a
+    run at rtol 1e-10 among them): the runs below it come back from the FP64
+    twin family of the same launch and match an FP64 solve of those runs,
+    the others match the FP32 solve, in the caller's order."""
+    from test_hetero_emulated import _fp32_vdp_family
     from cubie_b200.hetero import FP32_RTOL_FLOOR, HeteroSolver
-    solvers, batches = families()
+    solvers, batches = _fp32_vdp_family()
     ts = np.array([1.0, 1e-3, 1.0, 1e-2, 0.5, 1.0, 1e-4])
     batches[1] = dict(batches[1], tol_scale=ts)
     hs = HeteroSolver(solvers)

@@ -47,12 +47,23 @@ def test_hetero_equals_separate_solves():
         assert o["totals"].tolist() == ref["totals"].tolist()
 
 
+def _fp32_vdp_family():
+    """The VdP family of ``families`` stepped in FP32 throughout."""
+    from cubie_b200 import Solver
+    solvers, batches = families()
+    s = solvers[1]
+    solvers[1] = Solver(s.system, algorithm="ros3p", rtol=1e-6, atol=1e-6, linear_correction_type="gmres",
+                        preconditioner_type=None, output_types=["state"])
+    return solvers, batches
+
+
 def test_fp32_floor_routes_tight_runs_to_an_fp64_twin():
     """Runs of an FP32 family whose rtol x tol_scale lies below the FP32
-    floor go to an FP64 twin family in the same launch (CPU: the routing
-    only)."""
-    from cubie_b200.hetero import FP32_RTOL_FLOOR, HeteroSolver
-    solvers, batches = families()
+    floor go to an FP64 twin family in the same launch; for a
+    mixed-precision family only runs below the (lower) mixed floor do (CPU:
+    the routing only)."""
+    from cubie_b200.hetero import FP32_RTOL_FLOOR, MIXED_RTOL_FLOOR, HeteroSolver
+    solvers, batches = _fp32_vdp_family()
     ts = np.array([1.0, 1e-3, 1.0, 1e-2, 0.5, 1.0, 1e-4])     # VdP rtol 1e-6 x scale
     batches[1] = dict(batches[1], tol_scale=ts)
     hs = HeteroSolver(solvers)
@@ -70,3 +81,8 @@ def test_fp32_floor_routes_tight_runs_to_an_fp64_twin():
     # the FP64 family (Robertson) and families without tight runs are untouched
     assert routes[0] == [(0, None)] and routes[2] == [(3, None)]
     assert HeteroSolver(solvers, fp32_floor=None).route(batches)[1][1] == [(1, None)]
+    # a mixed-precision family: only the run below the mixed floor (1e-10)
+    mixed, mb = families()
+    mb[1] = dict(mb[1], tol_scale=ts)
+    r = HeteroSolver(mixed).route(mb)[1][1]
+    assert [idx.tolist() for _, idx in r] == [[0, 1, 2, 3, 4, 5], [6]] and 1e-6 * 1e-4 < MIXED_RTOL_FLOOR

@@ -53,7 +53,8 @@ def test_gpu_matches_reference_fixture(cuda_device, name):
         assert tol_units(res.state, ref["state"], atol, rtol) < bar
         if "state_summaries" in ref.files:
             assert tol_units(res.state_summaries, ref["state_summaries"], atol, rtol) < bar
-    if "iteration_counters" in ref.files and case["precision"] == "float64":
+    if "iteration_counters" in ref.files and case["precision"] == "float64" and \
+            not case.get("counters_rounding_sensitive"):
         np.testing.assert_array_equal(res.iteration_counters[:, 2:, :], ref["iteration_counters"][:, 2:, :])
 
 
