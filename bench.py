@@ -141,6 +141,19 @@ class CpuReference:
         self.pool.join()
 
 
+def reference_simulator_record():
+    """The reference's own kernels under Numba's CUDA simulator on the first
+    8 runs of this workload, as recorded by
+    tests/golden/time_reference_simulator.py where the reference is
+    installed (it is not on a GPU host); reported beside the port."""
+    p = ROOT / "tests" / "golden" / "ref_simulator_timing.json"
+    if not p.exists():
+        return None
+    rec = json.loads(p.read_text())
+    return {k: rec[k] for k in ("value", "unit", "cores", "solved", "runs", "wall_s", "sample")} | {
+        "kind": "reference", "where": "recorded by tests/golden/time_reference_simulator.py, not on this host"}
+
+
 def cpu_reference(per_core: int = 2, max_steps: int = 3000, seed: int = SEED):
     """One timed pass of :class:`CpuReference`."""
     ref = CpuReference(per_core, max_steps, seed)
@@ -870,6 +883,8 @@ def gpu_arm(args, rank: int, world: int, dist):
         adj = adjoint_arm(args, dev) if args.adj_n > 0 else None
         log('adjoint', adj)
         cpu = cpu_reference(per_core=args.cpu_per_core, max_steps=args.cpu_max_steps) if not args.no_cpu else None
+        if cpu is not None:
+            cpu["reference_simulator_recorded"] = reference_simulator_record()
         v = variants
         factors = {
             "persistent_vs_plain_mixed": value / v["plain_mixed"]["value"],
@@ -988,6 +1003,8 @@ def main():
     ap.add_argument("--cpu-per-core", type=int, default=2)
     ap.add_argument("--cpu-max-steps", type=int, default=3000)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--block", type=int, default=128, help="block size of the headline launches")
+    ap.add_argument("--min-blocks", type=int, default=1, help="minimum resident blocks per SM (register cap)")
     ap.add_argument("--headline-only", action="store_true",
                     help="time the headline launch only and print its record (for profiling)")
     ap.add_argument("--ref-per-core", type=int, default=1, help="--impl reference: runs per core per pass")
@@ -1015,6 +1032,8 @@ def main():
     args = ap.parse_args()
     for cfg in (NEW, NEW_RADAU):
         cfg["linear_correction_type"] = args.linear
+        cfg["block_size"] = args.block
+        cfg["min_blocks_per_sm"] = args.min_blocks
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if args.impl == "reference":
