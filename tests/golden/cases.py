@@ -336,9 +336,6 @@ CASES.update({
                                 inputs=("rober", 3, 71), duration=0.5,
                                 kwargs=dict(dt=1e-3, rtol=1e-6, atol=1e-8, save_every=0.125,
                                             linear_correction_type="bicgstab", output_types=_ITS)),
-    "vdp_mass_ros3p_f64": dict(system=VDP_MASS, algorithm="ros3p", precision="float64",
-                               inputs=("vdp", 3, 73, [1.0, 3.0, 10.0]), duration=2.0,
-                               kwargs=dict(rtol=1e-7, atol=1e-7, save_every=0.5, output_types=_ITS)),
     "vdp_mass_radau_f32": dict(system=VDP_MASS, algorithm="radau", precision="float32",
                                inputs=("vdp", 3, 74, [1.0, 3.0, 10.0]), duration=2.0,
                                kwargs=dict(rtol=1e-6, atol=1e-6, save_every=0.5, output_types=_ITS)),
