@@ -287,6 +287,16 @@ struct RosenbrockStep {
                 if (!Tab::ACC_OUT && stage == Tab::B_ROW) ynew[i] = v;
                 if (Tab::HAS_ERR && !Tab::ACC_ERR && stage == Tab::BHAT_ROW) err[i] = v;
             }
+            if constexpr (Sys::HAS_MASS) {
+                // the C_ij K_j / h term of a mass-matrix system is
+                // M (C_ij K_j) / h (Hairer & Wanner, Solving ODEs II, VI.4;
+                // the reference leaves M out, generic_rosenbrock_w.py:682-698,
+                // and fails on every non-identity M tried)
+                R mc[N];
+                Sys::template mass_mv<R>(rhs, mc);
+#pragma unroll
+                for (int i = 0; i < N; ++i) rhs[i] = mc[i];
+            }
             if constexpr (ND > 0) {
                 if (stage == 0) {
 #pragma unroll

@@ -18,8 +18,8 @@ Followed files (reference, ``src/cubie/``):
   DIRK step        integrators/algorithms/generic_dirk.py:515-855
   mass matrix      odesystems/symbolic/codegen/linear_operators.py:708-735,
                    nonlinear_residuals.py:59-130,324-345 (M v and M u terms;
-                   Rosenbrock's C_ij k_j / h term without M, as the
-                   reference forms it: generic_rosenbrock_w.py:682-698)
+                   Rosenbrock's C_ij k_j / h term with M applied, where the
+                   reference, generic_rosenbrock_w.py:682-698, omits it)
   dense predictor  integrators/stage_predictors.py:76-548
   Newton           integrators/matrix_free_solvers/newton_krylov.py:340-517
   MR / SD          integrators/matrix_free_solvers/linear_solver.py:220-385
@@ -1082,7 +1082,11 @@ def integrate(system: OracleSystem, algorithm: str, inits: np.ndarray, params: n
                 for j in range(stage):
                     if tab.C[stage, j] != 0.0:
                         corr = corr + rt(tab.C[stage, j]) * Ks[j]
-                rv = fs + corr * inv_dt[:, None] + rt(tab.gamma_stages[stage]) * tdv
+                # with a mass matrix the C_ij K_j / h term is M (C_ij K_j) / h
+                # (Hairer & Wanner, Solving ODEs II, VI.4); the reference
+                # leaves M out of it (generic_rosenbrock_w.py:682-698), which
+                # no non-identity M we tried survives
+                rv = fs + system.mv(corr) * inv_dt[:, None] + rt(tab.gamma_stages[stage]) * tdv
                 rhs = rv * h[:, None] * gamma
                 x, st, li = lin_solve(A, Pc, nrm, rhs, Ks[stage - 1].copy())
                 step_status |= st
