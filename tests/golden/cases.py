@@ -294,9 +294,9 @@ CASES.update({
 # ``counters_rounding_sensitive`` marks a case whose step and iteration
 # counts follow last-bit differences (BiCGSTAB on a singular-mass stage
 # system): compared in tolerance units, not counter by counter.
-# ``slow_oracle`` marks cases whose FP32 Krylov iterations (tens of
-# thousands of minimal-residual or BiCGSTAB iterations per stiff run) take
-# the NumPy oracle minutes: their oracle pins run when CBX_SLOW_PINS=1, and
+# ``slow_oracle`` marks cases that take the NumPy oracle minutes (tens of
+# thousands of FP32 Krylov iterations per stiff run; the 256-state cable's
+# dense Jacobians): their oracle pins run when CBX_SLOW_PINS=1, and
 # the GPU tests compare them with the reference fixture only.
 _MU = ("vdp_manifold", [1.4, 1.2, 1.1], [100.0, 300.0, 1000.0])
 _HH_DRV = dict(seed=0, n_samples=1000, period=0.01, t0=0.0, order=3, wrap=False, boundary_condition="clamped",
@@ -316,7 +316,7 @@ CASES.update({
                                 kwargs=dict(rtol=1e-6, atol=1e-6, save_every=2.0, linear_correction_type="bicgstab",
                                             output_types=_ITS)),
     "hh64_dirk3_bicgstab_f32": dict(system=HH64, algorithm="l_stable_dirk_3", precision="float32",
-                                    inputs=("hh", 2, 60), duration=4.0, drivers=_HH_DRV,
+                                    inputs=("hh", 2, 60), duration=4.0, drivers=_HH_DRV, slow_oracle=True,
                                     engine=dict(layout="warp"),
                                     kwargs=dict(dt=0.025, rtol=1e-4, atol=1e-4, linear_correction_type="bicgstab",
                                                 save_every=0.5, summarise_every=4.0, sample_summaries_every=0.05,
