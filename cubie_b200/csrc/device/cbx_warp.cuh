@@ -89,7 +89,10 @@ struct WarpCtx {
         for (int q = 0; q < ND; ++q)
             if (lane == q) dst[q] = drv[q];
     }
-    // f(t, y): y and f local.
+    // f(t, y): y and f local.  Every exchange is put -> sync -> class code
+    // -> sync -> get: the second sync already orders every lane's reads of
+    // the inputs before any later put, and every write of ``out`` comes after
+    // the next exchange's first sync, so no sync follows the get.
     __device__ __forceinline__ void rhs(const R* yloc, R t, const R* drv, R* floc) const {
         put(m->ys, yloc);
         put_drivers(m->d, drv);
@@ -97,7 +100,6 @@ struct WarpCtx {
         Cfg::WSys::template dxdt_lanes<R>(m->ys, m->p, m->d, t, m->out, lane);
         __syncwarp();
         get(m->out, floc);
-        __syncwarp();
     }
     __device__ __forceinline__ void linearize(const R* Yloc, R t, const R* drv) const {
         if constexpr (CACHED) {
@@ -121,7 +123,6 @@ struct WarpCtx {
             Cfg::WSys::template fj_lanes<R>(m->ys, m->p, m->d, t, m->out, m->jac, lane);
             __syncwarp();
             get(m->out, floc);
-            __syncwarp();
         } else {
             rhs(Yloc, t, drv, floc);
             linearize(Yloc, t, drv);
@@ -138,7 +139,6 @@ struct WarpCtx {
         }
         __syncwarp();
         get(m->out, outloc);
-        __syncwarp();
     }
 };
 
