@@ -21,11 +21,24 @@ standard library and converts the MathML itself:
   ``e-notation`` and ``integer`` forms; ``pi``, ``exponentiale``, ``true``,
   ``false``, ``infinity``, ``notanumber``.
 
-Not done here: unit conversion (each variable is taken in the units its
-component declares, so connections between different but compatible
-units need the factor written into the model), ``reset`` and ``import``
-elements (both rejected with ``NotImplementedError``), and the reference's
-optional rewrite of removable
+Units: every unit resolves to a factor times a product of base units
+(the SI base and derived units, prefixes, exponents, multipliers,
+component-level and user-defined base units).  A model variable is held in
+the units of its defining occurrence; an occurrence in another component
+with compatible but different units reads it scaled by the ratio of the
+factors, and equations defining it there are scaled back (the reference
+converts through pint, cellmlmanip's units handling).  Incompatible units
+across a connection raise ``ValueError``; units with an offset (celsius)
+raise ``NotImplementedError``.
+
+Imports (CellML 1.1 and 2.0): components and units of other documents,
+found relative to the importing file; an imported component brings the
+components it encapsulates (named ``<local name>__<name>``) and the
+connections among them; imports may nest.  Both documents use the same
+CellML version.
+
+Not done here: ``reset`` elements (rejected with ``NotImplementedError``),
+and the reference's optional rewrite of removable
 Goldman-Hodgkin-Katz singularities (``U / (exp(U) - 1)`` is compiled as
 written; it is finite everywhere except exactly at ``U = 0``).
 
@@ -179,6 +192,183 @@ class _MathML:
         raise ValueError(f"unsupported MathML operator <{op}>")
 
 
+# --------------------------------------------------------------------------
+# units (CellML 1.0 section 5, CellML 2.0 section 9): a unit is a factor
+# times a product of base units; converting between compatible units of
+# connected variables scales by the ratio of their factors
+# --------------------------------------------------------------------------
+_PREFIX = {"yotta": 24, "zetta": 21, "exa": 18, "peta": 15, "tera": 12, "giga": 9, "mega": 6, "kilo": 3,
+           "hecto": 2, "deka": 1, "deca": 1, "deci": -1, "centi": -2, "milli": -3, "micro": -6, "nano": -9,
+           "pico": -12, "femto": -15, "atto": -18, "zepto": -21, "yocto": -24}
+
+
+def _u(factor=1.0, **dims):
+    return float(factor), {k: v for k, v in dims.items() if v}
+
+
+_BUILTIN_UNITS = {
+    "ampere": _u(A=1), "candela": _u(cd=1), "kelvin": _u(K=1), "kilogram": _u(kg=1), "metre": _u(m=1),
+    "meter": _u(m=1), "mole": _u(mol=1), "second": _u(s=1), "gram": _u(1e-3, kg=1), "dimensionless": _u(),
+    "radian": _u(), "steradian": _u(), "becquerel": _u(s=-1), "hertz": _u(s=-1), "coulomb": _u(s=1, A=1),
+    "farad": _u(m=-2, kg=-1, s=4, A=2), "gray": _u(m=2, s=-2), "sievert": _u(m=2, s=-2),
+    "henry": _u(m=2, kg=1, s=-2, A=-2), "joule": _u(m=2, kg=1, s=-2), "katal": _u(s=-1, mol=1),
+    "liter": _u(1e-3, m=3), "litre": _u(1e-3, m=3), "lumen": _u(cd=1), "lux": _u(m=-2, cd=1),
+    "newton": _u(m=1, kg=1, s=-2), "ohm": _u(m=2, kg=1, s=-3, A=-2), "pascal": _u(m=-1, kg=1, s=-2),
+    "siemens": _u(m=-2, kg=-1, s=3, A=2), "tesla": _u(kg=1, s=-2, A=-1), "volt": _u(m=2, kg=1, s=-3, A=-1),
+    "watt": _u(m=2, kg=1, s=-3), "weber": _u(m=2, kg=1, s=-2, A=-1),
+}
+
+
+class _Units:
+    """Unit definitions in scope for one component: its own, its model's,
+    and the built-in units."""
+
+    def __init__(self, defs: Dict[str, ET.Element], cml: str, parent: Optional["_Units"] = None):
+        self.defs, self.cml, self.parent = defs, cml, parent
+        self._cache: Dict[str, Tuple[float, Dict[str, float]]] = {}
+
+    def _find(self, name):
+        scope = self
+        while scope is not None:
+            if name in scope.defs:
+                return scope
+            scope = scope.parent
+        return None
+
+    def resolve(self, name: str, _depth: int = 0) -> Tuple[float, Dict[str, float]]:
+        if name in self._cache:
+            return self._cache[name]
+        scope = self._find(name)
+        if scope is None:
+            if name == "celsius":
+                raise NotImplementedError("units with an offset (celsius) are not converted")
+            if name not in _BUILTIN_UNITS:
+                raise ValueError(f"unknown units '{name}'")
+            return _BUILTIN_UNITS[name]
+        if _depth > 64:
+            raise ValueError(f"units '{name}' are defined in terms of themselves")
+        el = scope.defs[name]
+        if el.get("base_units") == "yes":
+            out = (1.0, {name: 1.0})
+        else:
+            factor, dims = 1.0, {}
+            for un in el.findall(scope.cml + "unit"):
+                if float(un.get("offset", "0") or 0) != 0.0:
+                    raise NotImplementedError(f"units '{name}': units with an offset are not converted")
+                f, d = scope.resolve(un.get("units"), _depth + 1)
+                pre = un.get("prefix", "0")
+                pexp = _PREFIX[pre] if pre in _PREFIX else int(pre)
+                e = float(un.get("exponent", "1"))
+                m = float(un.get("multiplier", "1"))
+                factor *= m * (10.0 ** pexp * f) ** e
+                for k, v in d.items():
+                    dims[k] = dims.get(k, 0.0) + v * e
+            out = (factor, {k: v for k, v in dims.items() if abs(v) > 1e-12})
+        self._cache[name] = out
+        return out
+
+
+def _scale(factor: float) -> sp.Expr:
+    """A unit-conversion factor as a SymPy number (exact for powers of ten
+    and other short decimals)."""
+    r = sp.nsimplify(repr(factor), rational=True)
+    return r if abs(float(r) - factor) <= 1e-15 * abs(factor) else sp.Float(repr(factor), 17)
+
+
+# --------------------------------------------------------------------------
+# imports (CellML 1.1 section 3, CellML 2.0 section 5): components and units
+# of other documents, with the components they encapsulate
+# --------------------------------------------------------------------------
+XLINK = "{http://www.w3.org/1999/xlink}href"
+
+
+def _encapsulation(root, cml: str) -> Dict[str, List[str]]:
+    """Parent -> children of the encapsulation hierarchy."""
+    children: Dict[str, List[str]] = {}
+
+    def walk(ref):
+        name = ref.get("component")
+        for sub in ref.findall(cml + "component_ref"):
+            children.setdefault(name, []).append(sub.get("component"))
+            walk(sub)
+
+    for grp in list(root.iter(cml + "group")) + list(root.iter(cml + "encapsulation")):
+        if grp.tag == cml + "group":
+            rels = [r.get("relationship") for r in grp.findall(cml + "relationship_ref")]
+            if "encapsulation" not in rels:
+                continue
+        for ref in grp.findall(cml + "component_ref"):
+            walk(ref)
+    return children
+
+
+def _flatten(path: Path, _seen: Tuple[str, ...] = ()):
+    """The model at ``path`` with its imports resolved: ``(cml namespace,
+    components {name: (element, units scope)}, connections [(c1, c2,
+    [(v1, v2), ...])], resets present)``.  Imported components keep the
+    local name the import gives them; the components they encapsulate are
+    brought along as ``<local name>__<their name>``."""
+    key = str(path.resolve())
+    if key in _seen:
+        raise ValueError(f"CellML import cycle through {path.name}")
+    doc = ET.parse(path).getroot()
+    ns = doc.tag[1:].split("}", 1)[0] if doc.tag.startswith("{") else ""
+    if ns not in CELLML_NS:
+        raise ValueError(f"not a CellML 1.0/1.1/2.0 model (root namespace '{ns}')")
+    cml = "{" + ns + "}"
+    v2 = ns.endswith("2.0#")
+    model_units = _Units({u.get("name"): u for u in doc.findall(cml + "units")}, cml)
+    comps: Dict[str, Tuple[ET.Element, _Units]] = {}
+    conns: List[Tuple[str, str, List[Tuple[str, str]]]] = []
+    resets = any(True for _ in doc.iter(cml + "reset"))
+    for imp in doc.findall(cml + "import"):
+        href = imp.get(XLINK)
+        if not href:
+            raise ValueError("CellML import without an xlink:href")
+        sub_ns, sub_comps, sub_conns, sub_resets = _flatten(path.parent / href, _seen + (key,))
+        resets = resets or sub_resets
+        sub_doc = ET.parse(path.parent / href).getroot()
+        sub_cml = "{" + sub_ns + "}"
+        tree = _encapsulation(sub_doc, sub_cml)
+        for iu in imp.findall(cml + ("import_units" if v2 else "units")):
+            ref = iu.get("units_ref")
+            defs = {u.get("name"): u for u in sub_doc.findall(sub_cml + "units")}
+            if ref not in defs:
+                raise ValueError(f"import of units '{ref}' from {href}: not defined there")
+            model_units.defs[iu.get("name")] = defs[ref]
+            # the imported definition's own references resolve among the
+            # imported document's units
+            model_units.defs.update({k: v for k, v in defs.items() if k not in model_units.defs})
+        for ic in imp.findall(cml + ("import_component" if v2 else "component")):
+            local, ref = ic.get("name"), ic.get("component_ref")
+            if ref not in sub_comps:
+                raise ValueError(f"import of component '{ref}' from {href}: not defined there")
+            names = {ref: local}
+            stack = [ref]
+            while stack:
+                parent = stack.pop()
+                for child in tree.get(parent, []):
+                    names[child] = f"{local}__{child}"
+                    stack.append(child)
+            for old, new in names.items():
+                comps[new] = sub_comps[old]
+            for c1, c2, pairs in sub_conns:
+                if c1 in names and c2 in names:
+                    conns.append((names[c1], names[c2], pairs))
+    for comp in doc.findall(cml + "component"):
+        local_units = {u.get("name"): u for u in comp.findall(cml + "units")}
+        comps[comp.get("name")] = (comp, _Units(local_units, cml, model_units) if local_units else model_units)
+    for conn in doc.findall(cml + "connection"):
+        if v2:
+            c1, c2 = conn.get("component_1"), conn.get("component_2")
+        else:
+            mc = conn.find(cml + "map_components")
+            c1, c2 = mc.get("component_1"), mc.get("component_2")
+        pairs = [(mv.get("variable_1"), mv.get("variable_2")) for mv in conn.findall(cml + "map_variables")]
+        conns.append((c1, c2, pairs))
+    return ns, comps, conns, resets
+
+
 def load_cellml_model(path, precision=np.float32, name: Optional[str] = None,
                       parameters: Optional[Sequence[str]] = None, observables: Optional[Sequence[str]] = None,
                       fix_singularities: bool = True, voltage_variable: Optional[str] = None,
@@ -198,40 +388,28 @@ def load_cellml_model(path, precision=np.float32, name: Optional[str] = None,
         raise ValueError(f"expected a .cellml file, got '{path.name}'")
     if show_gui:
         raise NotImplementedError("the constants editor GUI is not part of cubie_b200")
-    root = ET.parse(path).getroot()
-    ns = root.tag[1:].split("}", 1)[0] if root.tag.startswith("{") else ""
-    if ns not in CELLML_NS:
-        raise ValueError(f"not a CellML 1.0/1.1/2.0 model (root namespace '{ns}')")
+    ns, comp_els, connections, resets = _flatten(path)
     cml = "{" + ns + "}"
-    v2 = ns.endswith("2.0#")
-    if root.find(cml + "import") is not None:
-        raise NotImplementedError("CellML imports are not supported: flatten the model into one document first")
-    if any(True for _ in root.iter(cml + "reset")):
+    if resets:
         raise NotImplementedError("CellML reset rules are not supported")
 
     # variables per component
     comps: Dict[str, Dict[str, dict]] = {}
     uf = _UnionFind()
-    for comp in root.iter(cml + "component"):
-        cname = comp.get("name")
+    for cname, (comp, units) in comp_els.items():
         vars_ = {}
         for var in comp.findall(cml + "variable"):
-            vars_[var.get("name")] = {"initial": var.get("initial_value")}
+            vars_[var.get("name")] = {"initial": var.get("initial_value"), "units": var.get("units")}
             uf.find((cname, var.get("name")))
         comps[cname] = vars_
-    for conn in root.iter(cml + "connection"):
-        if v2:
-            c1, c2 = conn.get("component_1"), conn.get("component_2")
-        else:
-            mc = conn.find(cml + "map_components")
-            c1, c2 = mc.get("component_1"), mc.get("component_2")
-        for mv in conn.findall(cml + "map_variables"):
-            uf.union((c1, mv.get("variable_1")), (c2, mv.get("variable_2")))
+    for c1, c2, pairs in connections:
+        for v1, v2_ in pairs:
+            uf.union((c1, v1), (c2, v2_))
 
     # equations per component, before naming (definitions decide names)
     equations = []  # (component, kind, target local name, rhs element, time local name)
     for cname in comps:
-        comp = next(c for c in root.iter(cml + "component") if c.get("name") == cname)
+        comp = comp_els[cname][0]
         for math in comp.findall("{%s}math" % MATHML):
             for ap in math:
                 kids = list(ap)
@@ -293,14 +471,43 @@ def load_cellml_model(path, precision=np.float32, name: Optional[str] = None,
         except ValueError:  # CellML 2.0: a variable of the same component
             return initial(uf.find((c, val)))
 
+    # unit conversion: a model variable is held in the units of its
+    # defining occurrence; an occurrence in another component with other
+    # (compatible) units reads it scaled by k = f_source / f_occurrence
+    def unit_of(c, v):
+        return comp_els[c][1].resolve(comps[c][v]["units"] or "dimensionless")
+
+    def k(c, v):
+        root_ = uf.find((c, v))
+        sc, sv = sources[root_]
+        if (sc, sv) == (c, v) or (comps[sc][sv]["units"] == comps[c][v]["units"]
+                                  and comp_els[sc][1] is comp_els[c][1]):
+            return 1.0      # the same units in the same scope: nothing to convert (or resolve)
+        f_src, d_src = unit_of(*sources[root_])
+        f_occ, d_occ = unit_of(c, v)
+        if set(d_src) != set(d_occ) or any(abs(d_src[q] - d_occ[q]) > 1e-12 for q in d_src):
+            raise ValueError(f"variable '{v}' of component '{c}' is connected to '{sources[root_][1]}' of "
+                             f"'{sources[root_][0]}' with incompatible units")
+        return f_src / f_occ
+
+    def read(c, local):
+        kk = k(c, local)
+        sym = symbols[uf.find((c, local))]
+        return sym if kk == 1.0 else _scale(kk) * sym
+
     derivatives: Dict[str, sp.Expr] = {}
     assignments: List[Tuple[sp.Symbol, sp.Expr]] = []
     states: Dict[str, float] = {}
     algebraic = set()
-    for cname, kind, target, rhs, _ in equations:
-        conv = _MathML(lambda local, c=cname: symbols[uf.find((c, local))])
+    for cname, kind, target, rhs, tname in equations:
+        conv = _MathML(lambda local, c=cname: read(c, local))
         expr = conv.convert(rhs)
         root_ = uf.find((cname, target))
+        # d(k_x x)/d(k_t t) = rhs  ->  dx/dt = (k_t / k_x) rhs;  k_x x = rhs  ->  x = rhs / k_x
+        kx = k(cname, target)
+        kt = k(cname, tname) if kind == "ode" else 1.0
+        if kt / kx != 1.0:
+            expr = _scale(kt / kx) * expr
         if kind == "ode":
             sname = names[root_]
             if sname in derivatives:
@@ -344,5 +551,15 @@ def load_cellml_model(path, precision=np.float32, name: Optional[str] = None,
     return SymbolicODE(states=states, parameters=params, constants=consts, drivers=[], observables=obs_list,
                        assignments=aux + ders, derivatives=derivatives, precision=precision,
                        name=name or path.stem,
-                       source="cellml:" + hashlib.sha256(path.read_bytes()).hexdigest() + "|P" + ",".join(params)
+                       source="cellml:" + hashlib.sha256(_model_bytes(path)).hexdigest() + "|P" + ",".join(params)
                        + "|O" + ",".join(obs_list))
+
+
+def _model_bytes(path: Path) -> bytes:
+    """The document and every document it imports (the system's identity)."""
+    out = path.read_bytes()
+    root = ET.parse(path).getroot()
+    for imp in root.iter():
+        if _local(imp.tag) == "import" and imp.get(XLINK):
+            out += _model_bytes(path.parent / imp.get(XLINK))
+    return out

@@ -226,8 +226,122 @@ def test_cellml11_namespace_and_unsupported_elements(tmp_path):
     imported = v11.replace('<component name="environment">',
                            '<import xmlns:xlink="http://www.w3.org/1999/xlink" xlink:href="other.cellml"/>'
                            '<component name="environment">')
-    with pytest.raises(NotImplementedError, match="imports"):
+    with pytest.raises(FileNotFoundError):               # imports resolve relative to the file
         load_cellml_model(_write(tmp_path, imported, "imp.cellml"))
     reset = GATE_CELLML_20.replace("</component>", "<reset variable=\"x\" test_variable=\"x\" order=\"1\"/></component>")
     with pytest.raises(NotImplementedError, match="reset"):
         load_cellml_model(_write(tmp_path, reset, "reset.cellml"))
+
+
+UNITS_CELLML_11 = """<?xml version="1.0"?>
+<model xmlns="http://www.cellml.org/cellml/1.1#" xmlns:cellml="http://www.cellml.org/cellml/1.1#" name="units">
+  <units name="millisecond"><unit units="second" prefix="milli"/></units>
+  <units name="millivolt"><unit units="volt" prefix="milli"/></units>
+  <units name="per_volt"><unit units="volt" exponent="-1"/></units>
+  <component name="env">
+    <variable name="time" units="second" public_interface="out"/>
+  </component>
+  <component name="cell">
+    <variable name="time" units="millisecond" public_interface="in"/>
+    <variable name="V" units="millivolt" initial_value="-65" public_interface="out"/>
+    <variable name="Vrest" units="millivolt" initial_value="-80"/>
+    <variable name="tau" units="millisecond" initial_value="10"/>
+    <math xmlns="http://www.w3.org/1998/Math/MathML">
+      <apply><eq/><apply><diff/><bvar><ci>time</ci></bvar><ci>V</ci></apply>
+        <apply><divide/><apply><minus/><ci>Vrest</ci><ci>V</ci></apply><ci>tau</ci></apply></apply>
+    </math>
+  </component>
+  <component name="probe">
+    <variable name="V" units="volt" public_interface="in"/>
+    <variable name="Vv" units="volt"/>
+    <math xmlns="http://www.w3.org/1998/Math/MathML">
+      <apply><eq/><ci>Vv</ci><apply><times/><cn cellml:units="dimensionless">2</cn><ci>V</ci></apply></apply>
+    </math>
+  </component>
+  <connection><map_components component_1="env" component_2="cell"/>
+    <map_variables variable_1="time" variable_2="time"/></connection>
+  <connection><map_components component_1="cell" component_2="probe"/>
+    <map_variables variable_1="V" variable_2="V"/></connection>
+</model>
+"""
+
+
+def test_cellml_units_convert_across_connections(tmp_path):
+    """Time in seconds in one component and milliseconds in another, a
+    voltage in millivolts read as volts elsewhere: the model variable keeps
+    its defining occurrence's units and every other occurrence is scaled."""
+    from cubie_b200.cellml import load_cellml_model
+    ode = load_cellml_model(_write(tmp_path, UNITS_CELLML_11, "units.cellml"), precision=np.float64,
+                            observables=["Vv"])
+    V = sp.Symbol("V", real=True)
+    assert ode.state_names == ["V"] and ode.initial_values["V"] == -65.0
+    # dV/dt_ms = (Vrest - V) / tau_ms with t in seconds: 1000 x
+    dv = ode.derivatives["V"].subs({sp.Symbol("Vrest", real=True): -80.0, sp.Symbol("tau", real=True): 10.0})
+    assert sp.simplify(dv - 100 * (-80 - V)) == 0
+    vv = dict((str(a), e) for a, e in ode.assignments)["Vv"]
+    assert sp.simplify(vv - V / 500) == 0                  # 2 x (V mV in volts)
+    bad = UNITS_CELLML_11.replace('<variable name="V" units="volt" public_interface="in"/>',
+                                  '<variable name="V" units="second" public_interface="in"/>')
+    with pytest.raises(ValueError, match="incompatible units"):
+        load_cellml_model(_write(tmp_path, bad, "bad.cellml"), observables=["Vv"])
+
+
+LIB_CELLML_11 = """<?xml version="1.0"?>
+<model xmlns="http://www.cellml.org/cellml/1.1#" xmlns:cellml="http://www.cellml.org/cellml/1.1#" name="lib">
+  <units name="per_second"><unit units="second" exponent="-1"/></units>
+  <component name="decay">
+    <variable name="t" units="second" public_interface="in" private_interface="out"/>
+    <variable name="x" units="dimensionless" initial_value="2" public_interface="out"/>
+    <variable name="k" units="per_second" private_interface="in"/>
+    <math xmlns="http://www.w3.org/1998/Math/MathML">
+      <apply><eq/><apply><diff/><bvar><ci>t</ci></bvar><ci>x</ci></apply>
+        <apply><minus/><apply><times/><ci>k</ci><ci>x</ci></apply></apply></apply>
+    </math>
+  </component>
+  <component name="rate">
+    <variable name="k" units="per_second" initial_value="0.5" public_interface="out"/>
+  </component>
+  <group><relationship_ref relationship="encapsulation"/>
+    <component_ref component="decay"><component_ref component="rate"/></component_ref></group>
+  <connection><map_components component_1="decay" component_2="rate"/>
+    <map_variables variable_1="k" variable_2="k"/></connection>
+</model>
+"""
+
+MAIN_CELLML_11 = """<?xml version="1.0"?>
+<model xmlns="http://www.cellml.org/cellml/1.1#" xmlns:cellml="http://www.cellml.org/cellml/1.1#"
+       xmlns:xlink="http://www.w3.org/1999/xlink" name="main">
+  <import xlink:href="lib.cellml">
+    <component name="first_order" component_ref="decay"/>
+    <units name="per_second" units_ref="per_second"/>
+  </import>
+  <component name="env">
+    <variable name="time" units="second" public_interface="out"/>
+    <variable name="y" units="dimensionless" initial_value="1"/>
+    <variable name="x" units="dimensionless" public_interface="in"/>
+    <math xmlns="http://www.w3.org/1998/Math/MathML">
+      <apply><eq/><apply><diff/><bvar><ci>time</ci></bvar><ci>y</ci></apply><ci>x</ci></apply>
+    </math>
+  </component>
+  <connection><map_components component_1="env" component_2="first_order"/>
+    <map_variables variable_1="time" variable_2="t"/>
+    <map_variables variable_1="x" variable_2="x"/></connection>
+</model>
+"""
+
+
+def test_cellml_import_brings_the_encapsulated_components(tmp_path):
+    """A component imported from another document (CellML 1.1), with the
+    component it encapsulates and the connection between them."""
+    from cubie_b200.cellml import load_cellml_model
+    _write(tmp_path, LIB_CELLML_11, "lib.cellml")
+    ode = load_cellml_model(_write(tmp_path, MAIN_CELLML_11, "main.cellml"), precision=np.float64,
+                            parameters=["k"])
+    assert sorted(ode.state_names) == ["x", "y"] and ode.parameters == {"k": 0.5}
+    x, y, k = (sp.Symbol(n, real=True) for n in ("x", "y", "k"))
+    assert sp.simplify(ode.derivatives["x"] + k * x) == 0 and sp.simplify(ode.derivatives["y"] - x) == 0
+    cyc = LIB_CELLML_11.replace('name="lib">', 'name="lib" xmlns:xlink="http://www.w3.org/1999/xlink">'
+                                '<import xlink:href="main.cellml"/>')
+    _write(tmp_path, cyc, "lib.cellml")
+    with pytest.raises(ValueError, match="cycle"):
+        load_cellml_model(tmp_path / "main.cellml")
