@@ -925,9 +925,9 @@ def gpu_arm(args, rank: int, world: int, dist):
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak_fp32, "unit": "TFLOP/s",
                          "frac": achieved / peak_fp32,
                          # DRAM bytes of one launch: the ncu capture of this kernel at 262,144 runs
-                         # (profiles/cbx_integrate_persistent__ros3p_direct_vdp_262144.md: 5.26 MB read,
+                         # (profiles/cbx_integrate_persistent__ros3p_direct_vdp_262144.md: 7.35 MB read,
                          # 0 B written) scaled by the runs processed (traffic is per-run input and output)
-                         "traffic": 5.26e6 * n / 262144,
+                         "traffic": 7.35e6 * n / 262144,
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of this kernel at "
                                            "262,144 runs, scaled by runs to this launch",
                          "peak_source": "measured FP32 FMA probe (cbx_fp32_peak_probe) in this run",
