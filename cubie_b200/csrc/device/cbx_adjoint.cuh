@@ -388,8 +388,9 @@ struct RosenbrockAdjoint {
 
     static __device__ __forceinline__ void reverse(const StepCtx<Cfg>& ctx, const R* y, R t, R h, R* lam,
                                                    C* pbar) {
+        using Rhs = RosenbrockRhs<Cfg>;
         const R gamma = R(Tab::GAMMA);
-        const R inv_dt = R(1) / h;
+        const R inv_dt = Rhs::FOLDED ? R(0) : R(1) / h;
         const R* drv = nullptr;  // no drivers on this path
         R J[Sys::NJ];
         Sys::template jac<R>(y, ctx.p, drv, t, J);
@@ -409,17 +410,14 @@ struct RosenbrockAdjoint {
 #pragma unroll
                 for (int j = 0; j < S; ++j) {
                     if (j < s && Tab::a(s, j) != 0.0) v += R(Tab::a(s, j)) * K[j][i];
-                    if (j < s && Tab::Cm(s, j) != 0.0) c += R(Tab::Cm(s, j)) * K[j][i];
+                    if (j < s && Tab::Cm(s, j) != 0.0) c += R(Rhs::cm(s, j)) * K[j][i];
                 }
                 Y[s][i] = v;
                 corr[i] = c;
             }
             Sys::template dxdt<R>(Y[s], ctx.p, drv, stage_time, f);
 #pragma unroll
-            for (int i = 0; i < N; ++i) {
-                const R rv = (s > 0) ? f[i] + corr[i] * inv_dt : f[i];
-                rhs[i] = rv * h * gamma;
-            }
+            for (int i = 0; i < N; ++i) rhs[i] = Rhs::value(f[i], corr[i], s == 0, h, inv_dt, gamma * h, R(0));
             int it = 0;
             linear_solve<Cfg>(op, rhs, guess, it);
 #pragma unroll

@@ -9,17 +9,20 @@
 // step caps the gain at the safety factor, and an accepted step that was
 // truncated onto an output event keeps dt (freeze) and leaves the history
 // untouched.  STEP_TOO_SMALL is returned when dt * gain <= dt_min.
-// The step size, its clamp to [dt_min, dt_max] and the STEP_TOO_SMALL test
-// run in the control precision C (FP64 on the mixed-precision path).  The
-// error norm and the gain arithmetic run in the gain precision G, which is
-// C except on the mixed-precision path, where it is FP32: both only decide
-// acceptance and a factor clamped to [min_gain, max_gain] that then scales
-// the FP64 step size, and 24 bits resolve either far below the
-// tolerances the path is used at, while FP64 divisions and powers cost
-// many issue slots per step.  Out-of-range arguments behave alike in both
-// widths after the clamp (an FP32 overflow to inf gives a zero or infinite
-// factor where FP64 gives a tiny or huge one; non-finite norms map to 1e16
-// in both).
+// Precision on the mixed-precision path: the step size, its clamp to
+// [dt_min, dt_max], the STEP_TOO_SMALL test, the controller history of
+// step sizes and the error norm's reduction (the sum of squared ratios and
+// the acceptance test) run in the control precision C, FP64.  Each
+// component's ratio e_i / tol_i and the gain's powers run in the gain
+// precision G, FP32: e_i and y_i are FP32 values, so their ratio carries no
+// more information in FP64, and the gain is a factor clamped to
+// [min_gain, max_gain] before it scales the FP64 step size, so its last
+// bits only nudge dt, while FP64 divisions and powers cost many issue slots
+// per step.  Out-of-range arguments behave alike in both widths after the
+// clamp (an FP32 overflow to inf gives a zero or infinite factor where FP64
+// gives a tiny or huge one; non-finite norms map to 1e16 in both).  On the
+// FP32 and FP64 paths G = C = the system precision, in the reference's
+// order of operations.
 #pragma once
 #include "cbx_common.cuh"
 
@@ -35,29 +38,36 @@ struct Controller {
         G h0, h1;   // previous error norms (PI, PID); h1: previous norm (Gustafsson)
         C hdt;      // previous accepted step size (Gustafsson)
     };
-    // On the mixed-precision path Gustafsson's previous norm is kept as
-    // log2(max(norm, 1e-16)): both of its powers then come from one log2 of
-    // the current norm (no reference counterpart, so no bit pattern to keep).
+    // On the mixed-precision path Gustafsson's controller works in the log2
+    // domain: h1 holds log2(max(previous norm, 1e-16)) and h0 log2 of the
+    // previous accepted step size, so both candidate gains come from one
+    // log2 of the norm and one of the step size, and the smaller is raised
+    // with a single exp2 (no reference counterpart, so no bit pattern to
+    // keep).
     static constexpr bool LOG_GUS = Cfg::MIXED && Cfg::CTRL == CTRL_GUSTAFSSON;
+    static constexpr double LOG2_1EM16 = -53.150849518197795;   // log2(1e-16)
     static __device__ __forceinline__ void init(State& st) {
-        st.h0 = G(0);
-        st.h1 = LOG_GUS ? G(-53.150849518197795) : G(0);   // log2(1e-16)
+        st.h0 = LOG_GUS ? G(-1e30) : G(0);   // no accepted step yet
+        st.h1 = LOG_GUS ? G(LOG2_1EM16) : G(0);
         st.hdt = C(0);
     }
     static __device__ __forceinline__ G gpow(G a, G b) { return pow_t(a, b); }
-    static __device__ __forceinline__ G error_norm2(const R* ynew, const R* y, const R* err, C tol_scale) {
-        G nrm2 = G(0);
+    // One component's ratio max(|e|, 1e-16) / (atol + rtol s max(|y_new|, |y|)).
+    static __device__ __forceinline__ G error_ratio(R e_i, R ynew_i, R y_i, G atol, G rtol, G ts) {
+        const G e = pymax(G(absv(e_i)), G(1e-16));
+        const G tol = atol + rtol * ts * pymax(G(absv(ynew_i)), G(absv(y_i)));
+        return e / tol;
+    }
+    static __device__ __forceinline__ C error_norm2(const R* ynew, const R* y, const R* err, C tol_scale) {
+        C nrm2 = C(0);
         const G ts = G(tol_scale);
 #pragma unroll
         for (int i = 0; i < N; ++i) {
-            const G e = pymax(G(absv(err[i])), G(1e-16));
-            const G tol = G(Cfg::atol(i)) + G(Cfg::rtol(i)) * ts * pymax(G(absv(ynew[i])), G(absv(y[i])));
-            const G ratio = e / tol;
+            const C ratio = C(error_ratio(err[i], ynew[i], y[i], G(Cfg::atol(i)), G(Cfg::rtol(i)), ts));
             nrm2 += ratio * ratio;
         }
-        nrm2 = nrm2 * G(Cfg::CTL_INV_N);
-        if (is_nan(nrm2) || !is_finite(nrm2)) nrm2 = G(1e16);
-        return nrm2;
+        // non-finite norms map to 1e16 in update_with_norm
+        return nrm2 * C(Cfg::CTL_INV_N);
     }
     static __device__ __forceinline__ G finish_gain(G gain, bool accept) {
         gain = clampv(gain, G(Cfg::CTL_MIN_GAIN), G(Cfg::CTL_MAX_GAIN));
@@ -79,14 +89,15 @@ struct Controller {
     }
     // The same decision from an error norm computed elsewhere (the
     // warp-per-system path reduces it over the lanes).
-    static __device__ __forceinline__ int update_with_norm(C& dt, G nrm2, int niters, bool truncated, bool& accept,
+    static __device__ __forceinline__ int update_with_norm(C& dt, C nrm2_c, int niters, bool truncated, bool& accept,
                                                            State& st) {
         if constexpr (Cfg::CTRL == CTRL_FIXED) {
             accept = true;
             return SUCCESS;
         } else {
-            if (is_nan(nrm2) || !is_finite(nrm2)) nrm2 = G(1e16);
-            accept = nrm2 <= G(1);
+            if (is_nan(nrm2_c) || !is_finite(nrm2_c)) nrm2_c = C(1e16);
+            accept = nrm2_c <= C(1);
+            const G nrm2 = G(nrm2_c);
             const G safety = G(Cfg::CTL_SAFETY);
             G gain;
             bool commit_history = accept && !truncated;
@@ -116,16 +127,21 @@ struct Controller {
                 const G tmp = gain_numerator / denom;
                 const G fac = safety < tmp ? safety : tmp;
                 if constexpr (LOG_GUS) {
-                    // nrm2^-e and (nrm2^2 / prev)^-e from one log2; the step
-                    // ratio in the gain precision (an FP64 division costs
-                    // about as much as the rest of the update)
+                    // gain_basic = fac nrm2^-e and gain_gus = safety (dt /
+                    // dt_prev) (nrm2^2 / prev)^-e, both fac 2^x: the smaller
+                    // exponent is raised once.  log2(safety / fac) is zero
+                    // unless the Newton count lowered fac (a constant fold
+                    // when the step reports no Newton iterations).
                     const G l2 = log2_t(nrm2);
-                    const G lprev = pymax(st.h1, G(-53.150849518197795));
-                    const G gain_basic = fac * exp2_t(-expo * l2);
-                    const G gain_gus = safety * (G(dt) / G(dt_prev)) * exp2_t(-expo * (G(2) * l2 - lprev));
-                    gain = gain_gus < gain_basic ? gain_gus : gain_basic;
-                    gain = (accept && dt_prev > C(1e-16)) ? gain : gain_basic;
+                    const G ldt = log2_t(G(current_dt));
+                    const G lprev = pymax(st.h1, G(LOG2_1EM16));
+                    const G lsf = safety < tmp ? G(0) : log2_t(safety / tmp);
+                    const G x_basic = -expo * l2;
+                    const G x_gus = lsf + (ldt - st.h0) - expo * (G(2) * l2 - lprev);
+                    const bool use_gus = accept && st.h0 > G(LOG2_1EM16);
+                    gain = fac * exp2_t(use_gus && x_gus < x_basic ? x_gus : x_basic);
                     st.h1 = commit_history ? l2 : st.h1;
+                    st.h0 = commit_history ? ldt : st.h0;
                 } else {
                     const G err_prev = pymax(st.h1, G(1e-16));
                     const G gain_basic = G(fac * gpow(nrm2, -expo));

@@ -407,6 +407,15 @@ __device__ __forceinline__ int solve_gmres(const Op& op, typename Cfg::R* rhs,
 // inverse diagonal is kept so a solve costs K^2 multiply-adds.  A
 // Rosenbrock step factors once and solves every stage with the factors,
 // which is the reason W/Rosenbrock methods freeze their Jacobian.
+//
+// K = 2 is solved in closed form instead: m holds adj(A) / det(A), one
+// reciprocal and no pivot search per factorisation, two multiplies and two
+// multiply-adds per solve.  For 2 x 2 systems Cramer's rule is forward
+// stable (Higham, Accuracy and Stability of Numerical Algorithms, 2nd ed.,
+// sec. 1.10.1): its error is within a small multiple of cond(A) times the
+// unit roundoff, the bound partial pivoting gives, which is what a stage
+// increment needs.  A zero, non-finite or overflowing determinant fails
+// the factorisation as a zero pivot does.
 template <class R, int K>
 struct DenseLU {
     R m[K][K];
@@ -423,6 +432,17 @@ struct DenseLU {
             op.apply(e, col);
 #pragma unroll
             for (int i = 0; i < K; ++i) m[i][j] = col[i];
+        }
+        if constexpr (K == 2) {
+            const R a00 = m[0][0], a01 = m[0][1], a10 = m[1][0], a11 = m[1][1];
+            const R det = a00 * a11 - a01 * a10;
+            const R inv = R(1) / det;
+            ok = is_finite(det) && is_finite(inv);
+            m[0][0] = a11 * inv;
+            m[0][1] = -a01 * inv;
+            m[1][0] = -a10 * inv;
+            m[1][1] = a00 * inv;
+            return;
         }
         ok = true;
 #pragma unroll
@@ -462,6 +482,12 @@ struct DenseLU {
     }
     // x = A^-1 b (b is left untouched).
     __device__ __forceinline__ void solve(const R* b, R* x) const {
+        if constexpr (K == 2) {
+            const R b0 = b[0], b1 = b[1];
+            x[0] = m[0][0] * b0 + m[0][1] * b1;
+            x[1] = m[1][0] * b0 + m[1][1] * b1;
+            return;
+        }
         R y[K];
 #pragma unroll
         for (int i = 0; i < K; ++i) y[i] = b[i];

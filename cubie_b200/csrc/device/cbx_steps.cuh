@@ -185,13 +185,52 @@ struct ErkStep {
 // (I - gamma h J) K_i = gamma h (f(Y_i) + sum_j C_ij K_j / h + gamma_i h f_t)
 // with Y_i = y + sum_j a_ij K_j and the Jacobian frozen at the step start.
 // ---------------------------------------------------------------------------
+// The right-hand side of a Rosenbrock stage's linear system is
+// h gamma (f_s + sum_j C_sj K_j / h + gs_s h f_t)
+// (generic_rosenbrock_w.py:682-698).  Written in that order it costs a
+// division per step and two multiplies per component beyond the sums; with
+// gamma folded into the C coefficients it is h gamma f_s + sum_j (gamma
+// C_sj) K_j (+ gs_s h gamma (h f_t)): one multiply-add per component and no
+// division.  The folded form is used wherever no reference result is
+// compared bit for bit (the mixed-precision mode and direct stage solves);
+// elsewhere the reference's order is kept.
+template <class Cfg>
+struct RosenbrockRhs {
+    using R = typename Cfg::R;
+    using Tab = typename Cfg::Tab;
+    static constexpr bool FOLDED = Cfg::MIXED || Cfg::LIN == LIN_DIRECT;
+    // coefficient of K_j in stage s's correction sum
+    static __device__ __forceinline__ constexpr double cm(int s, int j) {
+        return FOLDED ? Tab::Cm(s, j) * Tab::GAMMA : Tab::Cm(s, j);
+    }
+    // one component: f the stage derivative, corr the correction sum (times
+    // M for a mass-matrix system), hg = gamma h, gs_tdv = gs_s (h f_t) or 0
+    static __device__ __forceinline__ R value(R f, R corr, bool first, R h, R inv_h, R hg, R gs_tdv) {
+        constexpr bool T = Cfg::Sys::HAS_DFDT;
+        if constexpr (FOLDED) {
+            R v = first ? f * hg : f * hg + corr;
+            if constexpr (T) v = v + gs_tdv * hg;
+            return v;
+        } else {
+            R rv = first ? f : f + corr * inv_h;
+            if constexpr (T) rv = rv + gs_tdv;
+            return rv * h * R(Tab::GAMMA);
+        }
+    }
+};
+
 template <class Cfg>
 struct RosenbrockStep {
     using R = typename Cfg::R;
     using C = typename Cfg::C;
     using Sys = typename Cfg::Sys;
     using Tab = typename Cfg::Tab;
+    using Rhs = RosenbrockRhs<Cfg>;
     static constexpr int N = Cfg::N, S = Cfg::S, ND = Cfg::ND;
+    // In the mixed-precision mode the proposed state only sizes the error
+    // tolerance (the state update is the compensated y + delta), so it is
+    // formed once from delta instead of accumulated beside it.
+    static constexpr bool YNEW_FROM_DELTA = Cfg::MIXED && Tab::ACC_OUT;
     struct Persist {
         R guess[N];   // last solved stage increment: first-stage initial guess
     };
@@ -204,7 +243,8 @@ struct RosenbrockStep {
                                                Iters& its) {
         its = Iters{};
         const R gamma = R(Tab::GAMMA);
-        const R inv_dt = R(1) / dt;
+        const R inv_dt = Rhs::FOLDED ? R(0) : R(1) / dt;
+        const R hg = gamma * dt;
         R J[Sys::NJ];
         Sys::template jac<R>(y, ctx.p, drv, t, J);
         // h times the time derivative of f (explicit t and driver chain
@@ -232,7 +272,7 @@ struct RosenbrockStep {
         R f[N], rhs[N], Y[N];
         R drv_stage[ND > 0 ? ND : 1];
         int status = SUCCESS;
-        SingleStageOp<Cfg> op{J, gamma * dt, y, ctx.tol_scale};
+        SingleStageOp<Cfg> op{J, hg, y, ctx.tol_scale};
         // direct solves: one factorisation of I - gamma h J serves every stage
         DenseLU<R, N> lu;
         if constexpr (Cfg::LIN == LIN_DIRECT) {
@@ -274,7 +314,7 @@ struct RosenbrockStep {
                     for (int q = 1; q < S; ++q) {
                         if (q == stage) {
                             a_sj = R(Tab::a(q, j));
-                            c_sj = R(Tab::Cm(q, j));
+                            c_sj = R(Rhs::cm(q, j));
                         }
                     }
                     if (j < stage) {
@@ -308,9 +348,9 @@ struct RosenbrockStep {
             Sys::template dxdt<R>(Y, ctx.p, ND > 0 ? drv_stage : drv, stage_time, f);
 #pragma unroll
             for (int i = 0; i < N; ++i) {
-                R rv = (stage > 0) ? f[i] + rhs[i] * inv_dt : f[i];
-                if constexpr (Sys::HAS_DFDT) rv = rv + gs_s * tdv[i];
-                rhs[i] = rv * dt * gamma;
+                R gs_tdv = R(0);
+                if constexpr (Sys::HAS_DFDT) gs_tdv = gs_s * tdv[i];
+                rhs[i] = Rhs::value(f[i], rhs[i], stage == 0, dt, inv_dt, hg, gs_tdv);
             }
             int it = 0;
             if constexpr (Cfg::LIN == LIN_DIRECT) {
@@ -327,9 +367,13 @@ struct RosenbrockStep {
                 for (int j = 0; j < S; ++j)
                     if (j == stage) K[j][i] = k;
                 delta[i] += b_s * k;
-                if (Tab::ACC_OUT) ynew[i] += b_s * k;
+                if (Tab::ACC_OUT && !YNEW_FROM_DELTA) ynew[i] += b_s * k;
                 if (Tab::HAS_ERR && Tab::ACC_ERR) err[i] += d_s * k;
             }
+        }
+        if constexpr (YNEW_FROM_DELTA) {
+#pragma unroll
+            for (int i = 0; i < N; ++i) ynew[i] = y[i] + delta[i];
         }
         if (Tab::HAS_ERR && !Tab::ACC_ERR) {
 #pragma unroll

@@ -193,20 +193,43 @@ struct WarpStageOp {
     __device__ __forceinline__ T reduce(T partial) const { return warp_sum(partial); }
 };
 
+// The per-lane vectors a stage solve starts from, passed by value into the
+// out-of-line solve (local placement): an address of the caller's arrays
+// crossing the call would put them, and every read of them in the Newton
+// loop, in local memory.
+template <class Cfg>
+struct WarpStageIn {
+    using R = typename Cfg::R;
+    static constexpr int L = WarpCtx<Cfg>::L, ND = Cfg::ND;
+    R base[L];                    // stage base state
+    R start[L];                   // step start state
+    R z[L];                       // initial guess of the stage increment
+    R drv[ND > 0 ? ND : 1];       // drivers at the stage time
+};
+template <class Cfg>
+struct WarpStageOut {
+    using R = typename Cfg::R;
+    using C = typename Cfg::C;
+    R z[WarpCtx<Cfg>::L];
+    C theta;
+    int status, newton, krylov;
+};
+
 // z = h f(t, base + a z) solved by Newton over the warp (DirkProblem).  The
 // base and step-start states are read through ``b(k)`` / ``y0(k)``: from
-// shared memory with the shared placement, from the caller's arrays
-// otherwise.
+// shared memory with the shared placement, from the problem's own copies
+// (registers) otherwise.
 template <class Cfg>
 struct WarpDirkProblem {
     using R = typename Cfg::R;
     using C = typename Cfg::C;
     static constexpr int K = WarpCtx<Cfg>::L;
     static constexpr int ND = Cfg::ND;
+    static constexpr int KL = Cfg::SHARED_SCRATCH ? 1 : K;
     static constexpr bool FUSED = true;
     WarpCtx<Cfg> w;   // by value: no address of the solve's state is taken
-    const R* base;
-    const R* step_start;
+    R base[KL];
+    R step_start[KL];
     R drv[ND > 0 ? ND : 1];
     R t, h, a;
     __device__ __forceinline__ R b(int k) const {
@@ -298,55 +321,84 @@ struct WarpDirkStep {
     // runs 24 % faster.  Moving the operator and norm helpers out of line
     // as well (98 KB) was slower again: their calls pass the per-lane
     // vectors through the stack.
-    // The context comes by value and the stage increment in a register
-    // array: passing the caller's context or increment by reference kept
-    // them in local memory, reloaded after every shared-memory store.  With
-    // the shared placement the increment crosses the call through shared
-    // memory; otherwise through ``z_io``.
-    static __device__ CBX_NOINLINE int stage_solve(WarpCtx<Cfg> w, const R* base, const R* y, const R* drv_stage,
-                                                      R stage_time, R dt, R a, R* z_io, C& theta, int2& iters) {
-        WarpDirkProblem<Cfg> prob{w, base, y, {}, stage_time, dt, a};
+    // The context comes by value, and with the local placement the stage
+    // base, step start, initial guess and drivers too (``WarpStageIn``),
+    // with the increment, theta and counts returned by value: passing the
+    // caller's arrays by address kept them in local memory, reloaded after
+    // every shared-memory store.  With the shared placement the base, step
+    // start and increment cross the call through shared memory.
+    static __device__ CBX_NOINLINE int stage_solve_shared(WarpCtx<Cfg> w, const R* drv_stage, R stage_time, R dt,
+                                                             R a, C& theta, int2& iters) {
+        WarpDirkProblem<Cfg> prob{w, {}, {}, {}, stage_time, dt, a};
 #pragma unroll
         for (int q = 0; q < ND; ++q) prob.drv[q] = drv_stage[q];
         prob.form_weights();
         R u[L];
 #pragma unroll
-        for (int k = 0; k < L; ++k) {
-            if constexpr (Cfg::SHARED_SCRATCH) u[k] = w.m->sz[w.lane + 32 * k];
-            else u[k] = z_io[k];
-        }
+        for (int k = 0; k < L; ++k) u[k] = w.m->sz[w.lane + 32 * k];
         C th = theta;
         int ni = 0, ki = 0;
         const int st = newton_solve<Cfg>(prob, u, th, ni, ki);
         theta = th;
 #pragma unroll
-        for (int k = 0; k < L; ++k) {
-            if constexpr (Cfg::SHARED_SCRATCH) w.m->sz[w.lane + 32 * k] = u[k];
-            else z_io[k] = u[k];
-        }
+        for (int k = 0; k < L; ++k) w.m->sz[w.lane + 32 * k] = u[k];
         iters = make_int2(ni, ki);
         return st;
     }
-    // With the shared placement the stage base goes to shared memory before
-    // the solve and no address of a per-lane array crosses the call, so those
-    // arrays stay in registers.
+    static __device__ CBX_NOINLINE WarpStageOut<Cfg> stage_solve_local(WarpCtx<Cfg> w, WarpStageIn<Cfg> in,
+                                                                        R stage_time, R dt, R a, C theta) {
+        WarpDirkProblem<Cfg> prob{w, {}, {}, {}, stage_time, dt, a};
+#pragma unroll
+        for (int k = 0; k < L; ++k) {
+            prob.base[k] = in.base[k];
+            prob.step_start[k] = in.start[k];
+        }
+#pragma unroll
+        for (int q = 0; q < ND; ++q) prob.drv[q] = in.drv[q];
+        prob.form_weights();
+        WarpStageOut<Cfg> out;
+#pragma unroll
+        for (int k = 0; k < L; ++k) out.z[k] = in.z[k];
+        out.theta = theta;
+        out.newton = 0;
+        out.krylov = 0;
+        out.status = newton_solve<Cfg>(prob, out.z, out.theta, out.newton, out.krylov);
+        return out;
+    }
     static __device__ __forceinline__ int solve_stage(WarpCtx<Cfg>& w, const R* base, const R* y,
                                                       const R* drv_stage, R stage_time, R dt, R a, Persist& ps,
                                                       Iters& its) {
-        int2 it2;
-        int st;
+        int ni, ki, st;
         if constexpr (Cfg::SHARED_SCRATCH) {
             w.put(w.m->sbase, base);
             w.put(w.m->sz, ps.z);
-            st = stage_solve(w, nullptr, nullptr, drv_stage, stage_time, dt, a, nullptr, ps.theta, it2);
+            int2 it2;
+            st = stage_solve_shared(w, drv_stage, stage_time, dt, a, ps.theta, it2);
             w.get(w.m->sz, ps.z);
+            ni = it2.x;
+            ki = it2.y;
         } else {
-            st = stage_solve(w, base, y, drv_stage, stage_time, dt, a, ps.z, ps.theta, it2);
+            WarpStageIn<Cfg> in;
+#pragma unroll
+            for (int k = 0; k < L; ++k) {
+                in.base[k] = base[k];
+                in.start[k] = y[k];
+                in.z[k] = ps.z[k];
+            }
+#pragma unroll
+            for (int q = 0; q < ND; ++q) in.drv[q] = drv_stage[q];
+            const WarpStageOut<Cfg> out = stage_solve_local(w, in, stage_time, dt, a, ps.theta);
+#pragma unroll
+            for (int k = 0; k < L; ++k) ps.z[k] = out.z[k];
+            ps.theta = out.theta;
+            st = out.status;
+            ni = out.newton;
+            ki = out.krylov;
         }
-        its.nit = it2.x;
-        its.kit = it2.y;
-        its.nit_all += it2.x;
-        its.kit_all += it2.y;
+        its.nit = ni;
+        its.kit = ki;
+        its.nit_all += ni;
+        its.kit_all += ki;
         return st;
     }
     static __device__ __forceinline__ int step(WarpCtx<Cfg>& w, const R* y, R* ynew, R* delta, R* err,
@@ -681,21 +733,21 @@ __device__ __forceinline__ bool warp_iterate(WarpLane<Cfg>& L, WarpCtx<Cfg>& w, 
     L.irrecoverable = L.irrecoverable || (!Cfg::ADAPTIVE && step_failed);
     bool accept;
     if constexpr (Cfg::ADAPTIVE) {
-        // error norm over the warp (Controller::error_norm2), in the gain
-        // precision G
+        // error norm over the warp (Controller::error_norm2): ratios in the
+        // gain precision G, their squares summed in the control precision
         using G = typename Cfg::G;
-        G nrm2 = G(0);
+        using Ctl = Controller<Cfg>;
+        C nrm2 = C(0);
         const G ts = G(w.tol_scale);
 #pragma unroll
         for (int i = 0; i < NL; ++i) {
             if (!w.valid(i)) continue;
             const int c = w.lane + 32 * i;
-            const G e = step_failed ? G(1e16) : pymax(G(absv(err[i])), G(1e-16));
-            const G tol = G(Cfg::atol(c)) + G(Cfg::rtol(c)) * ts * pymax(G(absv(ynew[i])), G(absv(L.y[i])));
-            const G ratio = e / tol;
+            const R e = step_failed ? R(1e16) : err[i];
+            const C ratio = C(Ctl::error_ratio(e, ynew[i], L.y[i], G(Cfg::atol(c)), G(Cfg::rtol(c)), ts));
             nrm2 += ratio * ratio;
         }
-        nrm2 = warp_sum(nrm2) * G(Cfg::CTL_INV_N);
+        nrm2 = warp_sum(nrm2) * C(Cfg::CTL_INV_N);
         bool ctl_accept = false;
         const int ctl_status = Controller<Cfg>::update_with_norm(L.dt, nrm2, nit, truncated, ctl_accept, L.ctl);
         accept = ctl_accept && !step_failed;

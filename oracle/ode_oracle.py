@@ -1050,9 +1050,19 @@ def integrate(system: OracleSystem, algorithm: str, inits: np.ndarray, params: n
             tdv = system.dfdt(tt, Y, P) * h[:, None]
             with np.errstate(divide="ignore"):
                 inv_dt = rt(1) / h
-            A, Pc, nrm = single_op(J, (gamma * h).astype(rt), Y)
+            hg = (gamma * h).astype(rt)
+            A, Pc, nrm = single_op(J, hg, Y)
             fy = system.f(tt, Y, P)
-            rhs = ((fy + rt(tab.gamma_stages[0]) * tdv) * h[:, None]) * gamma
+            # The engine folds gamma into the C coefficients where no
+            # reference result is compared bit for bit (mixed precision,
+            # direct stage solves): h gamma f + sum_j (gamma C_sj) K_j
+            # (+ gs h gamma (h f_t)), the same sum in another order.
+            folded = mixed or S.linear_correction_type == "direct"
+            if folded:
+                # (f_t is zero for autonomous systems: the term adds nothing)
+                rhs = fy * hg[:, None] + (rt(tab.gamma_stages[0]) * tdv) * hg[:, None]
+            else:
+                rhs = ((fy + rt(tab.gamma_stages[0]) * tdv) * h[:, None]) * gamma
             Ks = []
             # the reference's Rosenbrock step never copies its Krylov count
             # into the step counters, so the reported counts stay zero
@@ -1081,13 +1091,17 @@ def integrate(system: OracleSystem, algorithm: str, inits: np.ndarray, params: n
                 corr = np.zeros((B, n), rt)
                 for j in range(stage):
                     if tab.C[stage, j] != 0.0:
-                        corr = corr + rt(tab.C[stage, j]) * Ks[j]
+                        cm = tab.C[stage, j] * tab.gamma if folded else tab.C[stage, j]
+                        corr = corr + rt(cm) * Ks[j]
                 # with a mass matrix the C_ij K_j / h term is M (C_ij K_j) / h
                 # (Hairer & Wanner, Solving ODEs II, VI.4); the reference
                 # leaves M out of it (generic_rosenbrock_w.py:682-698), which
                 # no non-identity M we tried survives
-                rv = fs + system.mv(corr) * inv_dt[:, None] + rt(tab.gamma_stages[stage]) * tdv
-                rhs = rv * h[:, None] * gamma
+                if folded:
+                    rhs = fs * hg[:, None] + system.mv(corr) + (rt(tab.gamma_stages[stage]) * tdv) * hg[:, None]
+                else:
+                    rv = fs + system.mv(corr) * inv_dt[:, None] + rt(tab.gamma_stages[stage]) * tdv
+                    rhs = rv * h[:, None] * gamma
                 x, st, li = lin_solve(A, Pc, nrm, rhs, Ks[stage - 1].copy())
                 step_status |= st
                 Ks.append(x)
@@ -1097,6 +1111,10 @@ def integrate(system: OracleSystem, algorithm: str, inits: np.ndarray, params: n
                 if bhrow is None:
                     err = err + rt(tab.d[stage]) * x
             ros_guess = np.where(act[:, None], Ks[-1], ros_guess)
+            if mixed and brow is None:
+                # the engine's mixed mode forms the proposed state (which
+                # only sizes the error tolerance) once from delta
+                ynew = Y + delta
             if tab.has_err and bhrow is not None:
                 err = ynew - err
         elif tab.kind == "firk":
