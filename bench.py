@@ -1023,7 +1023,7 @@ def main():
                     help="algorithm of the mixed batch's Van der Pol family")
     ap.add_argument("--c3-n", type=int, default=65536, help="Hodgkin-Huxley cable leg size (0: skip)")
     ap.add_argument("--c3-steps", type=int, default=2)
-    ap.add_argument("--c3-placement", default="auto", choices=["shared", "local", "auto"],
+    ap.add_argument("--c3-placement", default="auto", choices=["shared", "local", "registers", "auto"],
                     help="stage-solve scratch placement of the cable's warp kernel")
     ap.add_argument("--c3-max-registers", type=int, default=0, help="register cap of the cable's warp kernel "
                     "(0: the compiler's default)")

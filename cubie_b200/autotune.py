@@ -4,7 +4,7 @@ For one solver configuration it compiles the kernel at a set of launch
 shapes (block size, i.e. warps per block, and a minimum of resident blocks
 per SM, which caps registers per thread) and, for the warp-per-system
 layout, scratch placements (the stage solve's scratch vectors in the warp's
-shared memory or in the lanes' registers and local memory; the reference
+shared memory, in the lanes' local memory, or passed in registers; the reference
 makes the same shared-versus-local choice per buffer with a fixed table,
 src/cubie/integrators/memory_heuristics.py:99-116), times the persistent
 launch of each on a sample of the caller's batch with CUDA events, and
@@ -36,9 +36,12 @@ DEFAULT_CANDIDATES: Tuple[Tuple[int, int], ...] = ((128, 1), (64, 1), (256, 1), 
 
 
 # warp-per-system layout: fewer shapes (each compile of a large system is
-# costly), each with both scratch placements
+# costly), each with the scratch placements; the register cap matters for
+# the placements that pass vectors by address (with "registers" the call
+# keeps them live and the compiler takes what it needs)
 WARP_CANDIDATES: Tuple[Tuple[int, int, str, int], ...] = tuple(
-    (b, 1, p, r) for b in (128, 64) for p in ("shared", "local") for r in (0, 168))
+    (b, 1, p, r) for b in (128, 64) for p in ("shared", "local") for r in (0, 168)) + tuple(
+    (b, 1, "registers", 0) for b in (128, 64))
 
 
 # runs of the caller's batch timed per candidate
@@ -68,7 +71,10 @@ def config_key(solver, duration: float, gpu_name: str) -> str:
     variant.max_registers = 0
     variant.__dict__["_prepared"] = {}
     src = variant.prepare(duration, load=False)["gen"].source
-    return hashlib.sha256((src + gpu_name).encode()).hexdigest()[:24]
+    # the device headers are included by path: their contents are part of
+    # the configuration's identity too
+    from . import _native
+    return hashlib.sha256((src + _native._headers_digest() + gpu_name).encode()).hexdigest()[:24]
 
 
 def choose(timings: Dict[Tuple, float]) -> Tuple:

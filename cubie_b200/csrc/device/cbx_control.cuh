@@ -58,9 +58,8 @@ struct Controller {
         const G tol = atol + rtol * ts * pymax(G(absv(ynew_i)), G(absv(y_i)));
         return e / tol;
     }
-    static __device__ __forceinline__ C error_norm2(const R* ynew, const R* y, const R* err, C tol_scale) {
+    static __device__ __forceinline__ C error_norm2(const R* ynew, const R* y, const R* err, G ts) {
         C nrm2 = C(0);
-        const G ts = G(tol_scale);
 #pragma unroll
         for (int i = 0; i < N; ++i) {
             const C ratio = C(error_ratio(err[i], ynew[i], y[i], G(Cfg::atol(i)), G(Cfg::rtol(i)), ts));
@@ -78,13 +77,14 @@ struct Controller {
         return accept ? gain : pymin(gain, G(Cfg::CTL_SAFETY));
     }
     // Returns the controller status bits; updates dt, accept and history.
+    // ``ts``: the run's tolerance scale in the gain precision
     static __device__ __forceinline__ int update(C& dt, const R* ynew, const R* y, const R* err, int niters,
-                                                 bool truncated, bool& accept, State& st, C tol_scale) {
+                                                 bool truncated, bool& accept, State& st, G ts) {
         if constexpr (Cfg::CTRL == CTRL_FIXED) {
             accept = true;
             return SUCCESS;
         } else {
-            return update_with_norm(dt, error_norm2(ynew, y, err, tol_scale), niters, truncated, accept, st);
+            return update_with_norm(dt, error_norm2(ynew, y, err, ts), niters, truncated, accept, st);
         }
     }
     // The same decision from an error norm computed elsewhere (the
@@ -95,9 +95,10 @@ struct Controller {
             accept = true;
             return SUCCESS;
         } else {
-            if (is_nan(nrm2_c) || !is_finite(nrm2_c)) nrm2_c = C(1e16);
+            // a NaN or infinite norm rejects the step; the gain sees 1e16
             accept = nrm2_c <= C(1);
-            const G nrm2 = G(nrm2_c);
+            G nrm2 = G(nrm2_c);
+            if (!is_finite(nrm2)) nrm2 = G(1e16);
             const G safety = G(Cfg::CTL_SAFETY);
             G gain;
             bool commit_history = accept && !truncated;

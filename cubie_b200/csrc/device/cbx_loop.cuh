@@ -37,6 +37,7 @@ struct Lane {
     C dt, dt_raw;
     C next_save, next_update;
     C tol_scale;
+    typename Cfg::G ctl_ts;   // tol_scale in the gain precision (the error norm's)
     R y[N];
     R comp[N];
     R p[NP > 0 ? NP : 1];
@@ -134,6 +135,7 @@ __device__ __forceinline__ void lane_begin(Lane<Cfg>& L, const cbx_solve_args a,
     L.run = run;
     const double duration = a.durations ? a.durations[run] : a.duration;
     L.tol_scale = a.tol_scale ? C(a.tol_scale[run]) : C(1);
+    L.ctl_ts = typename Cfg::G(L.tol_scale);
     L.t = a.t0;
     L.tp = C(L.t);
     L.t_end = C(a.warmup + a.t0 + duration);
@@ -302,7 +304,7 @@ __device__ __forceinline__ bool lane_iterate(Lane<Cfg>& L, const cbx_solve_args 
     if constexpr (Cfg::ADAPTIVE) {
         bool ctl_accept = false;
         const int ctl_status =
-            Controller<Cfg>::update(L.dt, ynew, L.y, err, nit, truncated, ctl_accept, L.ctl, L.tol_scale);
+            Controller<Cfg>::update(L.dt, ynew, L.y, err, nit, truncated, ctl_accept, L.ctl, L.ctl_ts);
         accept = ctl_accept && !step_failed;
         L.iteration_status |= ctl_status;
         L.irrecoverable = L.irrecoverable || ((ctl_status & STEP_TOO_SMALL) != 0);

@@ -194,9 +194,10 @@ struct WarpStageOp {
 };
 
 // The per-lane vectors a stage solve starts from, passed by value into the
-// out-of-line solve (local placement): an address of the caller's arrays
-// crossing the call would put them, and every read of them in the Newton
-// loop, in local memory.
+// out-of-line solve ("registers" placement): no address of the caller's
+// arrays crosses the call, so neither they nor the Newton loop's reads of
+// them go to local memory, at the price of more live registers around the
+// call.
 template <class Cfg>
 struct WarpStageIn {
     using R = typename Cfg::R;
@@ -217,28 +218,32 @@ struct WarpStageOut {
 
 // z = h f(t, base + a z) solved by Newton over the warp (DirkProblem).  The
 // base and step-start states are read through ``b(k)`` / ``y0(k)``: from
-// shared memory with the shared placement, from the problem's own copies
-// (registers) otherwise.
+// shared memory with the "shared" placement, from the problem's own copies
+// with "registers", from the caller's arrays (local memory) with "local".
 template <class Cfg>
 struct WarpDirkProblem {
     using R = typename Cfg::R;
     using C = typename Cfg::C;
     static constexpr int K = WarpCtx<Cfg>::L;
     static constexpr int ND = Cfg::ND;
-    static constexpr int KL = Cfg::SHARED_SCRATCH ? 1 : K;
+    static constexpr int KL = Cfg::REG_SCRATCH ? K : 1;
     static constexpr bool FUSED = true;
     WarpCtx<Cfg> w;   // by value: no address of the solve's state is taken
-    R base[KL];
-    R step_start[KL];
+    const R* base_p;
+    const R* start_p;
+    R base_v[KL];
+    R start_v[KL];
     R drv[ND > 0 ? ND : 1];
     R t, h, a;
     __device__ __forceinline__ R b(int k) const {
         if constexpr (Cfg::SHARED_SCRATCH) return w.valid(k) ? w.m->sbase[w.lane + 32 * k] : R(0);
-        else return base[k];
+        else if constexpr (Cfg::REG_SCRATCH) return base_v[k];
+        else return base_p[k];
     }
     __device__ __forceinline__ R y0(int k) const {
         if constexpr (Cfg::SHARED_SCRATCH) return w.valid(k) ? w.m->sstart[w.lane + 32 * k] : R(0);
-        else return step_start[k];
+        else if constexpr (Cfg::REG_SCRATCH) return start_v[k];
+        else return start_p[k];
     }
     __device__ __forceinline__ void residual(const R* z, R* out) const {
         R Y[K], f[K];
@@ -321,37 +326,45 @@ struct WarpDirkStep {
     // runs 24 % faster.  Moving the operator and norm helpers out of line
     // as well (98 KB) was slower again: their calls pass the per-lane
     // vectors through the stack.
-    // The context comes by value, and with the local placement the stage
-    // base, step start, initial guess and drivers too (``WarpStageIn``),
-    // with the increment, theta and counts returned by value: passing the
-    // caller's arrays by address kept them in local memory, reloaded after
-    // every shared-memory store.  With the shared placement the base, step
-    // start and increment cross the call through shared memory.
-    static __device__ CBX_NOINLINE int stage_solve_shared(WarpCtx<Cfg> w, const R* drv_stage, R stage_time, R dt,
-                                                             R a, C& theta, int2& iters) {
-        WarpDirkProblem<Cfg> prob{w, {}, {}, {}, stage_time, dt, a};
+    // The context comes by value: passing the caller's context by reference
+    // kept it in local memory, reloaded after every shared-memory store.
+    // The stage base, step start and increment cross the call through
+    // shared memory ("shared" placement), by address from the caller's
+    // arrays ("local": they live in local memory, cached in L1, and the
+    // kernel body keeps few registers), or by value with the increment,
+    // theta and counts returned by value ("registers": no local memory for
+    // them, more live registers around the call).  The autotuner picks.
+    static __device__ CBX_NOINLINE int stage_solve(WarpCtx<Cfg> w, const R* base, const R* y, const R* drv_stage,
+                                                      R stage_time, R dt, R a, R* z_io, C& theta, int2& iters) {
+        WarpDirkProblem<Cfg> prob{w, base, y, {}, {}, {}, stage_time, dt, a};
 #pragma unroll
         for (int q = 0; q < ND; ++q) prob.drv[q] = drv_stage[q];
         prob.form_weights();
         R u[L];
 #pragma unroll
-        for (int k = 0; k < L; ++k) u[k] = w.m->sz[w.lane + 32 * k];
+        for (int k = 0; k < L; ++k) {
+            if constexpr (Cfg::SHARED_SCRATCH) u[k] = w.m->sz[w.lane + 32 * k];
+            else u[k] = z_io[k];
+        }
         C th = theta;
         int ni = 0, ki = 0;
         const int st = newton_solve<Cfg>(prob, u, th, ni, ki);
         theta = th;
 #pragma unroll
-        for (int k = 0; k < L; ++k) w.m->sz[w.lane + 32 * k] = u[k];
+        for (int k = 0; k < L; ++k) {
+            if constexpr (Cfg::SHARED_SCRATCH) w.m->sz[w.lane + 32 * k] = u[k];
+            else z_io[k] = u[k];
+        }
         iters = make_int2(ni, ki);
         return st;
     }
-    static __device__ CBX_NOINLINE WarpStageOut<Cfg> stage_solve_local(WarpCtx<Cfg> w, WarpStageIn<Cfg> in,
-                                                                        R stage_time, R dt, R a, C theta) {
-        WarpDirkProblem<Cfg> prob{w, {}, {}, {}, stage_time, dt, a};
+    static __device__ CBX_NOINLINE WarpStageOut<Cfg> stage_solve_regs(WarpCtx<Cfg> w, WarpStageIn<Cfg> in,
+                                                                       R stage_time, R dt, R a, C theta) {
+        WarpDirkProblem<Cfg> prob{w, nullptr, nullptr, {}, {}, {}, stage_time, dt, a};
 #pragma unroll
         for (int k = 0; k < L; ++k) {
-            prob.base[k] = in.base[k];
-            prob.step_start[k] = in.start[k];
+            prob.base_v[k] = in.base[k];
+            prob.start_v[k] = in.start[k];
         }
 #pragma unroll
         for (int q = 0; q < ND; ++q) prob.drv[q] = in.drv[q];
@@ -369,15 +382,7 @@ struct WarpDirkStep {
                                                       const R* drv_stage, R stage_time, R dt, R a, Persist& ps,
                                                       Iters& its) {
         int ni, ki, st;
-        if constexpr (Cfg::SHARED_SCRATCH) {
-            w.put(w.m->sbase, base);
-            w.put(w.m->sz, ps.z);
-            int2 it2;
-            st = stage_solve_shared(w, drv_stage, stage_time, dt, a, ps.theta, it2);
-            w.get(w.m->sz, ps.z);
-            ni = it2.x;
-            ki = it2.y;
-        } else {
+        if constexpr (Cfg::REG_SCRATCH) {
             WarpStageIn<Cfg> in;
 #pragma unroll
             for (int k = 0; k < L; ++k) {
@@ -387,13 +392,25 @@ struct WarpDirkStep {
             }
 #pragma unroll
             for (int q = 0; q < ND; ++q) in.drv[q] = drv_stage[q];
-            const WarpStageOut<Cfg> out = stage_solve_local(w, in, stage_time, dt, a, ps.theta);
+            const WarpStageOut<Cfg> out = stage_solve_regs(w, in, stage_time, dt, a, ps.theta);
 #pragma unroll
             for (int k = 0; k < L; ++k) ps.z[k] = out.z[k];
             ps.theta = out.theta;
             st = out.status;
             ni = out.newton;
             ki = out.krylov;
+        } else {
+            int2 it2;
+            if constexpr (Cfg::SHARED_SCRATCH) {
+                w.put(w.m->sbase, base);
+                w.put(w.m->sz, ps.z);
+                st = stage_solve(w, nullptr, nullptr, drv_stage, stage_time, dt, a, nullptr, ps.theta, it2);
+                w.get(w.m->sz, ps.z);
+            } else {
+                st = stage_solve(w, base, y, drv_stage, stage_time, dt, a, ps.z, ps.theta, it2);
+            }
+            ni = it2.x;
+            ki = it2.y;
         }
         its.nit = ni;
         its.kit = ki;

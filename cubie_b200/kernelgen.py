@@ -104,7 +104,9 @@ class KernelSpec:
     layout: str = "thread"
     # where the warp layout keeps its stage-solve scratch vectors (stage
     # base, step start, BiCGSTAB shadow residual): "shared" memory of the
-    # warp, or "local" (the lane's registers, spilling to local memory)
+    # warp, "local" (the lane's arrays, passed by address into the
+    # out-of-line stage solve, so in local memory) or "registers" (passed
+    # and returned by value)
     scratch_placement: str = "local"
     # register cap per thread passed to the compiler (0: its default)
     max_registers: int = 0
@@ -353,6 +355,8 @@ def family_block(system: SymbolicODE, spec: KernelSpec, gen: GeneratedSystem, ns
         f"    static constexpr int MIN_BLOCKS = {max(int(spec.min_blocks_per_sm), 1)};",
         f"    static constexpr bool SHARED_SCRATCH = "
         f"{str(spec.layout == 'warp' and spec.scratch_placement == 'shared').lower()};",
+        f"    static constexpr bool REG_SCRATCH = "
+        f"{str(spec.layout == 'warp' and spec.scratch_placement == 'registers').lower()};",
         f"    using Step = {STEP_TYPES[tab.kind]};",
         *([f"    using WSys = {ns}::WarpSystem;"] if warp_source is not None else []),
         *accessors,

@@ -156,12 +156,14 @@ class Solver:
                 raise NotImplementedError("the warp-per-system layout takes systems without a mass matrix")
             if execution.get("adjoint"):
                 raise NotImplementedError("the discrete adjoint takes systems without a mass matrix")
-        # warp layout: stage-solve scratch vectors in "shared" memory or
-        # "local" (registers / local memory; the faster of the two on the
-        # 256-state cable); "auto" lets the autotuner pick
+        # warp layout: stage-solve scratch vectors in "shared" memory,
+        # "local" (the lanes' arrays in local memory, cached in L1; the
+        # fastest on the 256-state cable at 65,536 runs) or "registers"
+        # (passed by value, more registers per thread); "auto" lets the
+        # autotuner pick
         sp_ = str(execution.get("scratch_placement", "local"))
-        if sp_ not in ("shared", "local", "auto"):
-            raise ValueError("scratch_placement must be 'shared', 'local' or 'auto'")
+        if sp_ not in ("shared", "local", "registers", "auto"):
+            raise ValueError("scratch_placement must be 'shared', 'local', 'registers' or 'auto'")
         self.placement_pending = sp_ == "auto"
         self.scratch_placement = "shared" if sp_ == "auto" else sp_
         # register cap per thread for the compiler (0: its default); the

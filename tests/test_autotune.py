@@ -67,7 +67,7 @@ def test_warp_layout_tunes_scratch_placement(tmp_path, monkeypatch):
                output_types=["state"])
     assert s.placement_pending and s.scratch_placement == "shared"
     cands = default_candidates(s)
-    assert {c[2] for c in cands} == {"shared", "local"} and all(len(c) == 4 for c in cands)
+    assert {c[2] for c in cands} == {"shared", "local", "registers"} and all(len(c) == 4 for c in cands)
     seen = []
 
     def fake(v):
@@ -83,3 +83,9 @@ def test_warp_layout_tunes_scratch_placement(tmp_path, monkeypatch):
                    output_types=["state"])
     assert "SHARED_SCRATCH = false" in fixed.prepare(2.0, load=False)["gen"].source
     assert "SHARED_SCRATCH = true" in s.prepare(2.0, load=False)["gen"].source
+    regs = Solver(sysm, algorithm="l_stable_dirk_3", layout="warp", scratch_placement="registers",
+                  output_types=["state"])
+    src = regs.prepare(2.0, load=False)["gen"].source
+    assert "REG_SCRATCH = true" in src and "SHARED_SCRATCH = false" in src
+    with pytest.raises(ValueError):
+        Solver(sysm, algorithm="l_stable_dirk_3", layout="warp", scratch_placement="texture")

@@ -82,3 +82,27 @@ def test_full_cable_warp_layout(cuda_device):
     assert np.all(vmax < 80.0) and np.all(vmean > -100.0) and np.all(vmean < 60.0)
     assert np.mean(vmax[0] > 0.0) > 0.5
     assert r.totals["newton"] > 0 and r.totals["krylov"] > 0
+
+
+@pytest.mark.parametrize("prec", [np.float64, np.float32])
+def test_scratch_placements_agree(cuda_device, prec):
+    """The three stage-solve scratch placements ("shared", "local",
+    "registers") run the same arithmetic on the 16-compartment cable: same
+    statuses and iteration totals, states within a small fraction of the
+    tolerance (the compiler may fuse a multiply-add differently in each)."""
+    nc, n, T = 16, 64, 10.0
+    x0, p = _inputs(nc, n, 3)
+    tol = 1e-8 if prec == np.float64 else 1e-4
+    kw = dict(rtol=tol, atol=tol, output_types=["state"], save_every=1.0, dt=0.025,
+              mixed_precision=prec == np.float32)
+    res = {}
+    for place in ("shared", "local", "registers"):
+        s = _solver(nc, prec, "warp", scratch_placement=place, **kw)
+        res[place] = s.solve(x0, p, drivers=_drivers(), duration=T, nan_error_trajectories=False)
+    ref = res["local"]
+    assert ref.status_codes.tolist() == [0] * n
+    bar = 1e-3 if prec == np.float64 else 1.0
+    for place in ("shared", "registers"):
+        r = res[place]
+        assert r.status_codes.tolist() == ref.status_codes.tolist()
+        assert _tol_units(r.state, ref.state, tol, tol) < bar, place
