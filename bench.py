@@ -814,7 +814,10 @@ def gpu_arm(args, rank: int, world: int, dist):
         gc.enable()
     log('e2e', e2e_times)
     e2e_frac, _ = solved_fraction(res.state[-1][:, :T], res.status_codes[:T])
-    e2e_s, e2e_solved = aggregate(float(np.mean(e2e_times)), n * e2e_frac, device=dev)
+    # the median step: a wall-clock step of the host API can be stretched
+    # many times over by host-side jitter outside the library (one 148 ms
+    # step among nineteen of 18 ms was seen); the mean is reported beside it
+    e2e_s, e2e_solved = aggregate(float(np.median(e2e_times)), n * e2e_frac, device=dev)
     e2e_value = e2e_solved / e2e_s
     h2d = x0_h.numel() * 4 + mu_h.numel() * 4 + du_h.numel() * 8
     d2h = res.state.size * 4 + res.status_codes.size * 4 + 4 * 8
@@ -920,7 +923,9 @@ def gpu_arm(args, rank: int, world: int, dist):
                        "l2": "flushed (256 MB write) before every timed launch",
                        "block": new["block"]},
             "e2e": {"value": e2e_value, "unit": "systems/s", "h2d_bytes_per_step": int(h2d),
-                    "d2h_bytes_per_step": int(d2h), "ms_per_step": 1e3 * float(np.mean(e2e_times))},
+                    "d2h_bytes_per_step": int(d2h), "ms_per_step": 1e3 * float(np.median(e2e_times)),
+                    "ms_per_step_mean": 1e3 * float(np.mean(e2e_times)),
+                    "statistic": "median of the timed wall-clock steps"},
             "gpu_launches": args.steps,
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak_fp32, "unit": "TFLOP/s",
                          "frac": achieved / peak_fp32,

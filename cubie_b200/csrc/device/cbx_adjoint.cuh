@@ -410,7 +410,7 @@ struct RosenbrockAdjoint {
 #pragma unroll
                 for (int j = 0; j < S; ++j) {
                     if (j < s && Tab::a(s, j) != 0.0) v += R(Tab::a(s, j)) * K[j][i];
-                    if (j < s && Tab::Cm(s, j) != 0.0) c += R(Rhs::cm(s, j)) * K[j][i];
+                    if (j < s && Tab::Cm(s, j) != 0.0) c += R(Tab::Cm(s, j)) * K[j][i];
                 }
                 Y[s][i] = v;
                 corr[i] = c;

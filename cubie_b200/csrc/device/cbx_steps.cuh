@@ -188,27 +188,28 @@ struct ErkStep {
 // The right-hand side of a Rosenbrock stage's linear system is
 // h gamma (f_s + sum_j C_sj K_j / h + gs_s h f_t)
 // (generic_rosenbrock_w.py:682-698).  Written in that order it costs a
-// division per step and two multiplies per component beyond the sums; with
-// gamma folded into the C coefficients it is h gamma f_s + sum_j (gamma
-// C_sj) K_j (+ gs_s h gamma (h f_t)): one multiply-add per component and no
-// division.  The folded form is used wherever no reference result is
+// division per step and two multiplies per component beyond the sums;
+// distributed, h gamma f_s + gamma sum_j C_sj K_j (+ gs_s h gamma (h f_t)),
+// it costs one multiply and one multiply-add per component and no
+// division.  The distributed form is used wherever no reference result is
 // compared bit for bit (the mixed-precision mode and direct stage solves);
-// elsewhere the reference's order is kept.
+// elsewhere the reference's order is kept.  gamma stays a separate factor:
+// folding it into the C coefficients would save the multiply, but the
+// products gamma C_sj rounded to FP32 perturb the method's coefficients
+// against the gamma of the stage matrix, and over the thousands of steps of
+// a tight-tolerance run in the mixed-precision mode that coherent error
+// doubled the 90th-percentile global error.
 template <class Cfg>
 struct RosenbrockRhs {
     using R = typename Cfg::R;
     using Tab = typename Cfg::Tab;
     static constexpr bool FOLDED = Cfg::MIXED || Cfg::LIN == LIN_DIRECT;
-    // coefficient of K_j in stage s's correction sum
-    static __device__ __forceinline__ constexpr double cm(int s, int j) {
-        return FOLDED ? Tab::Cm(s, j) * Tab::GAMMA : Tab::Cm(s, j);
-    }
-    // one component: f the stage derivative, corr the correction sum (times
-    // M for a mass-matrix system), hg = gamma h, gs_tdv = gs_s (h f_t) or 0
+    // one component: f the stage derivative, corr = sum_j C_sj K_j (times M
+    // for a mass-matrix system), hg = gamma h, gs_tdv = gs_s (h f_t) or 0
     static __device__ __forceinline__ R value(R f, R corr, bool first, R h, R inv_h, R hg, R gs_tdv) {
         constexpr bool T = Cfg::Sys::HAS_DFDT;
         if constexpr (FOLDED) {
-            R v = first ? f * hg : f * hg + corr;
+            R v = first ? f * hg : f * hg + R(Tab::GAMMA) * corr;
             if constexpr (T) v = v + gs_tdv * hg;
             return v;
         } else {
@@ -314,7 +315,7 @@ struct RosenbrockStep {
                     for (int q = 1; q < S; ++q) {
                         if (q == stage) {
                             a_sj = R(Tab::a(q, j));
-                            c_sj = R(Rhs::cm(q, j));
+                            c_sj = R(Tab::Cm(q, j));
                         }
                     }
                     if (j < stage) {

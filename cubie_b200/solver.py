@@ -15,8 +15,9 @@ through the C ABI (:mod:`cubie_b200._native`).  Device buffers are torch
 tensors; the library only receives their pointers.
 
 Additions beyond the reference are opt-in keywords:
-``mixed_precision`` (FP32 stepping with FP64 time, control and norms and a
-compensated state update), ``kernel`` (``"persistent"`` work-stealing launch
+``mixed_precision`` (FP32 stepping with FP64 time, step size, error-norm
+reduction and Newton norms, the gain's powers in FP32, and a compensated
+state update), ``kernel`` (``"persistent"`` work-stealing launch
 or the ``"plain"`` one-thread-per-run launch), ``linear_correction_type=
 "gmres"``, per-run ``durations`` and ``tol_scale`` arrays, ``max_steps``.
 """

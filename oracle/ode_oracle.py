@@ -1053,10 +1053,10 @@ def integrate(system: OracleSystem, algorithm: str, inits: np.ndarray, params: n
             hg = (gamma * h).astype(rt)
             A, Pc, nrm = single_op(J, hg, Y)
             fy = system.f(tt, Y, P)
-            # The engine folds gamma into the C coefficients where no
-            # reference result is compared bit for bit (mixed precision,
-            # direct stage solves): h gamma f + sum_j (gamma C_sj) K_j
-            # (+ gs h gamma (h f_t)), the same sum in another order.
+            # The engine distributes h gamma where no reference result is
+            # compared bit for bit (mixed precision, direct stage solves):
+            # h gamma f + gamma sum_j C_sj K_j (+ gs h gamma (h f_t)), the
+            # same sum in another order.
             folded = mixed or S.linear_correction_type == "direct"
             if folded:
                 # (f_t is zero for autonomous systems: the term adds nothing)
@@ -1091,14 +1091,13 @@ def integrate(system: OracleSystem, algorithm: str, inits: np.ndarray, params: n
                 corr = np.zeros((B, n), rt)
                 for j in range(stage):
                     if tab.C[stage, j] != 0.0:
-                        cm = tab.C[stage, j] * tab.gamma if folded else tab.C[stage, j]
-                        corr = corr + rt(cm) * Ks[j]
+                        corr = corr + rt(tab.C[stage, j]) * Ks[j]
                 # with a mass matrix the C_ij K_j / h term is M (C_ij K_j) / h
                 # (Hairer & Wanner, Solving ODEs II, VI.4); the reference
                 # leaves M out of it (generic_rosenbrock_w.py:682-698), which
                 # no non-identity M we tried survives
                 if folded:
-                    rhs = fs * hg[:, None] + system.mv(corr) + (rt(tab.gamma_stages[stage]) * tdv) * hg[:, None]
+                    rhs = fs * hg[:, None] + gamma * system.mv(corr) + (rt(tab.gamma_stages[stage]) * tdv) * hg[:, None]
                 else:
                     rv = fs + system.mv(corr) * inv_dt[:, None] + rt(tab.gamma_stages[stage]) * tdv
                     rhs = rv * h[:, None] * gamma
