@@ -16,11 +16,14 @@ from .interpolator import ArrayInterpolator
 from .adjoint import AdjointIntegrator, solve_ivp_adjoint
 from .autotune import autotune
 from .cellml import load_cellml_model
+from .structural import (ExtraEquationsSystemError, ExtraVariablesSystemError, InvalidSystemError,
+                         structural_simplify)
 
 __version__ = "0.1.0"
 
 __all__ = [
-    "load_cellml_model",
+    "load_cellml_model", "structural_simplify", "InvalidSystemError", "ExtraEquationsSystemError",
+    "ExtraVariablesSystemError",
     "CUBIE_RESULT_CODES", "decode_status_codes", "SymbolicODE", "create_ODE_system",
     "Solver", "solve_ivp", "SolveResult", "SolveSpec", "TABLEAU_REGISTRY", "Tableau",
     "resolve_algorithm", "GraphSolve", "ArrayInterpolator", "AdjointIntegrator", "solve_ivp_adjoint", "autotune",

@@ -17,6 +17,7 @@ Python) and turned into SymPy expressions.
 from __future__ import annotations
 
 import ast
+import re
 import hashlib
 from typing import Callable, Dict, Iterable, List, Mapping, Optional, Sequence, Tuple, Union
 
@@ -317,6 +318,9 @@ def create_ODE_system(
     name: Optional[str] = None,
     strict: bool = False,
     mass=None,
+    simplify: Optional[bool] = None,
+    state_priority: Optional[Mapping[str, float]] = None,
+    irreducible: Optional[Iterable[str]] = None,
     **unsupported,
 ) -> SymbolicODE:
     """Build a :class:`SymbolicODE` from ``lhs = rhs`` equation strings.
@@ -331,6 +335,17 @@ def create_ODE_system(
     order; ``None`` is the identity), as the reference's ``mass`` argument:
     a singular M makes a semi-explicit DAE and needs an implicit
     algorithm.
+
+    DAE input (an implicit equation ``0 = g`` or ``expr = expr``, a
+    declared state without a derivative equation or defined explicitly,
+    a second derivative ``d(d(x, t), t) = f``), or ``simplify=True``, goes
+    through :func:`cubie_b200.structural.structural_simplify` first, as
+    the reference's ``simplify`` path does (``symbolicODE.py:380-470``):
+    aliases and solvable algebraic unknowns become observables, the
+    remaining algebraic unknowns stay as states with their residuals, and
+    the system carries the mass matrix diag(1, ..., 1, 0, ..., 0), which a
+    caller's ``mass`` cannot override.  ``state_priority`` and
+    ``irreducible`` steer which unknowns survive.
     """
     for key, value in unsupported.items():
         if value not in (None, False, {}):
@@ -346,6 +361,13 @@ def create_ODE_system(
     else:
         driver_names = list(drivers) if drivers is not None else []
     obs_names = list(observables) if observables is not None else []
+    if simplify is not False and (simplify or _is_dae_input(eqs, state_defaults)):
+        if mass is not None:
+            raise ValueError("the system's mass matrix is derived by structural simplification and pairs with "
+                             "the simplified state order; 'mass' cannot override it")
+        return _create_dae_system(eqs, precision, state_defaults, obs_names, param_defaults, const_defaults,
+                                  driver_names, driver_settings, name, strict, state_priority or {},
+                                  list(irreducible or ()))
 
     lhs_names = [lhs for lhs, _ in eqs]
     # derivative targets
@@ -423,6 +445,141 @@ def create_ODE_system(
                        observables=obs_names, assignments=assignments,
                        derivatives=derivatives, precision=precision, name=name,
                        driver_settings=driver_settings, source=source, mass=mass)
+
+
+_SECOND = re.compile(r"^d\(\s*d\(\s*([A-Za-z_]\w*)\s*,\s*t\s*\)\s*,\s*t\s*\)$")
+_FIRST = re.compile(r"^d\(\s*([A-Za-z_]\w*)\s*,\s*t\s*\)$")
+
+
+def _is_dae_input(eqs, state_defaults) -> bool:
+    """Whether the equations need structural simplification: an implicit
+    or higher-order left-hand side, an explicit definition of a declared
+    state, or a declared state without a derivative equation."""
+    have_deriv = set()
+    for lhs, _ in eqs:
+        if _SECOND.match(lhs) or _FIRST.match(lhs):
+            return True
+        if not lhs.isidentifier():
+            return True
+        if lhs in state_defaults:
+            return True
+        if lhs.startswith("d") and lhs[1:] in state_defaults:
+            have_deriv.add(lhs[1:])
+    return bool(state_defaults) and any(s not in have_deriv for s in state_defaults)
+
+
+def _create_dae_system(eqs, precision, state_defaults, obs_names, param_defaults, const_defaults, driver_names,
+                       driver_settings, name, strict, state_priority, irreducible) -> "SymbolicODE":
+    """The DAE front end of :func:`create_ODE_system` (structural
+    simplification, then an implicit system with a singular mass matrix)."""
+    from .structural import structural_simplify
+    if not state_defaults:
+        raise ValueError("DAE input needs its unknowns declared as states")
+    symbols: Dict[str, sp.Symbol] = {}
+    unknowns = {n: symbols.setdefault(n, sp.Symbol(n, real=True)) for n in state_defaults}
+    inputs = set(param_defaults) | set(const_defaults) | set(driver_names)
+    derivs: Dict[sp.Symbol, sp.Expr] = {}
+    explicit: List[Tuple[sp.Symbol, sp.Expr]] = []
+    implicit: List[sp.Expr] = []
+    aux: List[Tuple[sp.Symbol, sp.Expr]] = []
+    order = list(state_defaults)
+    defaults = dict(state_defaults)
+
+    def set_derivative(target: str, expr: sp.Expr) -> None:
+        sym = unknowns[target]
+        if sym in derivs:
+            raise ValueError(f"state '{target}' has two derivative equations")
+        derivs[sym] = expr
+
+    for lhs, rhs in eqs:
+        expr = parse_expression(rhs, symbols)
+        m2, m1 = _SECOND.match(lhs), _FIRST.match(lhs)
+        target = m2.group(1) if m2 else (m1.group(1) if m1 else None)
+        if target is None and lhs.startswith("d") and lhs[1:] in unknowns:
+            target = lhs[1:]
+        if target is not None:
+            if target not in unknowns:
+                raise ValueError(f"'{lhs}' differentiates '{target}', which is not a declared state")
+            if m2:
+                # companion state for the first derivative (x_t, x_tt ...)
+                comp = f"{target}_t"
+                while comp in unknowns or comp in inputs or comp in symbols:
+                    comp += "_"
+                unknowns[comp] = symbols.setdefault(comp, sp.Symbol(comp, real=True))
+                order.insert(order.index(target) + 1, comp)
+                defaults.setdefault(comp, 0.0)
+                set_derivative(target, unknowns[comp])
+                set_derivative(comp, expr)
+            else:
+                set_derivative(target, expr)
+        elif lhs.isidentifier() and lhs in unknowns:
+            explicit.append((unknowns[lhs], expr))
+        elif lhs.isidentifier() and lhs not in inputs:
+            aux.append((symbols.setdefault(lhs, sp.Symbol(lhs, real=True)), expr))
+        elif lhs.isidentifier():
+            raise ValueError(f"'{lhs}' is declared as an input and is immutable")
+        else:
+            # ``lhs = rhs`` constrains rhs - lhs to zero (``0 = g`` gives g)
+            implicit.append(expr - parse_expression(lhs, symbols))
+    # auxiliary definitions (and references to a state's derivative) are
+    # substituted so that the structure is seen in the unknowns
+    dsyms = {symbols[f"d{n}"]: derivs[unknowns[n]] for n in unknowns
+             if f"d{n}" in symbols and unknowns[n] in derivs}
+    rule = {**{a: e for a, e in aux}, **dsyms}
+    for _ in range(len(rule) + 1):
+        new_rule = {k: v.xreplace(rule) for k, v in rule.items()}
+        if new_rule == rule:
+            break
+        rule = new_rule
+
+    def expand(e: sp.Expr) -> sp.Expr:
+        return e.xreplace(rule)
+
+    derivs = {k: expand(v) for k, v in derivs.items()}
+    explicit = [(u, expand(e)) for u, e in explicit]
+    implicit = [expand(g) for g in implicit]
+    known_names = set(unknowns) | inputs | {a.name for a, _ in aux} | {"t"}
+    used = set()
+    for e in list(derivs.values()) + [e for _, e in explicit] + implicit:
+        used |= {s.name for s in e.free_symbols}
+    undeclared = sorted(used - known_names)
+    if undeclared:
+        if strict:
+            raise ValueError(f"undefined symbols with strict=True: {undeclared}")
+        for u in undeclared:
+            param_defaults[u] = 0.0
+    for o in obs_names:
+        if o not in {a.name for a, _ in aux} and o not in unknowns:
+            raise ValueError(f"observable '{o}' has no defining equation")
+    res = structural_simplify([unknowns[n] for n in order], derivs, implicit, explicit,
+                              {unknowns[k]: float(v) for k, v in state_priority.items() if k in unknowns},
+                              [unknowns[k] for k in irreducible if k in unknowns])
+    states_out = {s.name: defaults[s.name] for s in res.states}
+    derivatives: Dict[str, sp.Expr] = {}
+    assignments: List[Tuple[sp.Symbol, sp.Expr]] = []
+    for s_ in res.differential_states:
+        derivatives[s_.name] = res.dxdt[s_]
+    for s_, g in zip(res.algebraic_states, res.residuals):
+        derivatives[s_.name] = g
+    observed_names = [u.name for u, _ in res.observed]
+    for u, e in res.observed:
+        assignments.append((u, e))
+    # the caller's auxiliaries, in terms of the surviving states
+    obs_rule = {u: e for u, e in res.observed}
+    for a, e in aux:
+        assignments.append((a, expand(e).xreplace(obs_rule)))
+    for n, e in derivatives.items():
+        assignments.append((sp.Symbol(f"d{n}", real=True), e))
+    seen = set(states_out) | set(param_defaults) | set(const_defaults) | set(driver_names) | {"t"}
+    assignments = _topological(assignments, seen)
+    observables_out = list(obs_names) + [n for n in observed_names if n not in obs_names]
+    source = "DAE|" + "\n".join(f"{l} = {r}" for l, r in eqs)
+    source += "|S" + ",".join(states_out) + "|P" + ",".join(param_defaults)
+    source += "|D" + ",".join(driver_names) + "|O" + ",".join(observables_out)
+    return SymbolicODE(states=states_out, parameters=param_defaults, constants=const_defaults,
+                       drivers=driver_names, observables=observables_out, assignments=assignments,
+                       derivatives=derivatives, precision=precision, name=name,
+                       driver_settings=driver_settings, source=source, mass=res.mass_matrix)
 
 
 def _topological(assignments, base_names):
