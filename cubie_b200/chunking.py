@@ -228,7 +228,8 @@ def run_chunked(solver, prep, inits, params, coeff_t, plan: ChunkPlan, duration,
                 slot.tol_d.copy_(slot.tol_h, non_blocking=True)
                 tol_t = slot.tol_d
             slot.bufs["totals"].zero_()
-            order = solver.run_order(dur_t) if dur_t is not None else None
+            order = solver.run_order(dur_t, tol_t[:m] if tol_t is not None else None) \
+                if dur_t is not None else None
             args = solver.make_args(prep, slot.bufs, slot.inits_d, slot.params_d, coeff_t, m, duration,
                                     settling_time, t0, slot.dur_d if dur_t is not None else None, tol_t,
                                     order_t=order, run_stride=chunk)

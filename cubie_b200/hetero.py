@@ -164,8 +164,8 @@ class HeteroSolver:
             dt = None if durs is None else torch.as_tensor(durs).to(device=dev, dtype=torch.float64).contiguous()
             ts = b.get("tol_scale")
             tt = None if ts is None else torch.as_tensor(ts).to(device=dev, dtype=torch.float64).contiguous()
-            # runs claimed longest horizon first within each family
-            order = s.run_order(dt) if dt is not None else None
+            # runs claimed by decreasing estimated work within each family
+            order = s.run_order(dt, tt) if dt is not None else None
             a = s.make_args(prep, bf, it, pt, None, n, duration, b.get("settling_time", 0.0), b.get("t0", 0.0),
                             dt, tt, order_t=order)
             keep.append(order)

@@ -675,7 +675,7 @@ class Solver:
         coeff_t = None
         if interp is not None:
             coeff_t = torch.as_tensor(interp.coefficients.astype(self.precision), device=dev).contiguous()
-        order_t = self.run_order(dur_t)
+        order_t = self.run_order(dur_t, tol_t)
         args = self.make_args(prep, bufs, inits_t, params_t, coeff_t, n_runs, duration, settling_time, t0,
                               dur_t, tol_t, order_t=order_t)
         kernel = self.launch_kind
@@ -723,16 +723,25 @@ class Solver:
         }
         return bufs
 
-    def run_order(self, dur_t):
+    def run_order(self, dur_t, tol_t=None):
         """Claim order of a persistent launch: with per-run horizons and
         ``schedule='longest_first'`` (the default ``'auto'`` when horizons
-        are given), the runs sorted by decreasing horizon, as a device
-        int64 permutation; otherwise None (claim in index order).  Each
-        run's result does not depend on the order."""
+        are given), the runs sorted by decreasing estimated work, as a
+        device int64 permutation; otherwise None (claim in index order).
+        The estimate is the horizon, times tol_scale^(-1/(q+1)) for an
+        adaptive method of order q when per-run tolerance scales are given
+        (an error-controlled step shrinks as the (q+1)-th root of the
+        tolerance), so a long, tight run is not claimed after shorter,
+        cheaper ones and left running alone at the end of the launch.
+        Each run's result does not depend on the order."""
         if dur_t is None or self.schedule == "index" or self.launch_kind == 0:
             return None
         torch = _torch()
-        return torch.argsort(dur_t, descending=True).to(torch.int64).contiguous()
+        cost = dur_t
+        if tol_t is not None and self.controller != "fixed":
+            q = max(int(getattr(self.tableau, "order", 1) or 1), 1)
+            cost = dur_t * torch.clamp(tol_t, min=1e-300) ** (-1.0 / (q + 1))
+        return torch.argsort(cost, descending=True).to(torch.int64).contiguous()
 
     def make_args(self, prep, bufs, inits_t, params_t, coeff_t, n_runs, duration, settling_time, t0,
                   dur_t=None, tol_t=None, max_steps=None, order_t=None,

@@ -89,3 +89,21 @@ def test_warp_layout_tunes_scratch_placement(tmp_path, monkeypatch):
     assert "REG_SCRATCH = true" in src and "SHARED_SCRATCH = false" in src
     with pytest.raises(ValueError):
         Solver(sysm, algorithm="l_stable_dirk_3", layout="warp", scratch_placement="texture")
+
+
+def test_claim_order_weighs_horizon_by_tolerance():
+    """Persistent launches claim runs by decreasing estimated work: the
+    horizon, times tol_scale^(-1/(q+1)) for an adaptive method of order q
+    when per-run tolerance scales are given; fixed steps ignore the scale."""
+    import torch
+    from cubie_b200 import Solver, create_ODE_system
+    sysm = create_ODE_system(VDP, states={"x": 2.0, "y": 0.0}, parameters={"mu": 10.0}, precision=np.float32)
+    s = Solver(sysm, algorithm="ros3p", output_types=["state"])      # order 3
+    dur = torch.tensor([10.0, 5.0, 1.0], dtype=torch.float64)
+    assert s.run_order(dur).tolist() == [0, 1, 2]
+    # 5 * (1e-8)^(-1/4) = 500 > 10 * 1 > 1 * (1e-2)^(-1/4) = 3.2
+    ts = torch.tensor([1.0, 1e-8, 1e-2], dtype=torch.float64)
+    assert s.run_order(dur, ts).tolist() == [1, 0, 2]
+    fixed = Solver(sysm, algorithm="l_stable_dirk_3", step_controller="fixed", dt=0.01, output_types=["state"])
+    assert fixed.run_order(dur, ts).tolist() == [0, 1, 2]
+    assert Solver(sysm, algorithm="ros3p", schedule="index", output_types=["state"]).run_order(dur, ts) is None
