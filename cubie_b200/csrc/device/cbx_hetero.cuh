@@ -11,11 +11,15 @@
 // ends), then moves on to the next family that still has runs; warps start
 // at different families (rotated by warp index) so all families progress
 // together and the launch ends when the last family's runs are done.
-// Within a family, claims follow its run_order when one is given (longest
-// horizon first, as in the single-family persistent launch).  Each
+// Within a family, claims follow its run_order when one is given (most
+// estimated work first, as in the single-family persistent launch).  Each
 // family's loop is its own function instantiation with its own loop state,
-// so the registers a lane needs are the most any one family needs, not the
-// sum.
+// value-initialised where it is declared: left uninitialised, its values
+// entered each family's loop undefined, and the compiler kept them live
+// across the loop over families, so the registers added up over the
+// families (124 for the three of the mixed batch, against 47 to 56 for
+// each alone).  Initialised, a lane needs about the most any one family
+// needs (64).
 #pragma once
 #include "cbx_loop.cuh"
 
@@ -23,7 +27,7 @@ namespace cbx {
 
 template <class Cfg>
 __device__ __forceinline__ void drain_family(const cbx_solve_args& a, unsigned long long* counter, BlockTotals* bt) {
-    Lane<Cfg> L;
+    Lane<Cfg> L{};
     bool active = false, exhausted = false;
     while (true) {
         if (!active && !exhausted) {
