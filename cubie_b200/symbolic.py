@@ -538,6 +538,15 @@ def _create_dae_system(eqs, precision, state_defaults, obs_names, param_defaults
     derivs = {k: expand(v) for k, v in derivs.items()}
     explicit = [(u, expand(e)) for u, e in explicit]
     implicit = [expand(g) for g in implicit]
+    # the derivative of an unknown with no derivative equation inside an
+    # expression makes a higher-index system
+    hidden = sorted(n for n in unknowns if unknowns[n] not in derivs and f"d{n}" in symbols
+                    and any(symbols[f"d{n}"] in e.free_symbols
+                            for e in list(derivs.values()) + [e for _, e in explicit] + implicit))
+    if hidden:
+        from .structural import InvalidSystemError
+        raise InvalidSystemError(f"derivatives of algebraic unknowns {hidden} appear in the equations (a "
+                                 "higher-index system); index reduction is not built")
     known_names = set(unknowns) | inputs | {a.name for a, _ in aux} | {"t"}
     used = set()
     for e in list(derivs.values()) + [e for _, e in explicit] + implicit:

@@ -103,6 +103,8 @@ def test_inconsistent_and_higher_index_systems_raise():
         create_ODE_system("dx = vx\ndy = vy\ndvx = T*x\ndvy = T*y - g\n0 = x**2 + y**2 - L**2",
                           states={"x": 1.0, "y": 0.0, "vx": 0.0, "vy": 0.0, "T": 0.0},
                           constants={"g": 9.81, "L": 1.0})
+    with pytest.raises(InvalidSystemError, match="derivatives of algebraic unknowns"):
+        create_ODE_system(["dx = -z", "0 = dz + x"], states={"x": 1.0, "z": 0.0})
     with pytest.raises(ValueError, match="immutable"):
         create_ODE_system(["k = 2*x", "0 = z - k", "dx = -z"], states={"x": 1.0, "z": 0.0},
                           parameters={"k": 0.5})
