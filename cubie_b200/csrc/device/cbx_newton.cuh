@@ -17,6 +17,28 @@ __device__ __forceinline__ typename Cfg::C krylov_tol(int i, typename Cfg::R ref
     return pymax(t, C(1e-16));
 }
 
+// One component's ratio v / max(atol + rtol scale |ref|, 1e-16) of a
+// tolerance-weighted norm; the caller sums the squares in the control
+// precision C.  On the mixed-precision path the ratio is formed in FP32:
+// v and ref are FP32 values, so the ratio carries no more information in
+// FP64, and an FP64 division per component costs more issue slots (and
+// code) than the rest of the norm.  Otherwise it is formed in C, in the
+// reference's order of operations.
+template <class Cfg>
+__device__ __forceinline__ typename Cfg::C tol_ratio(typename Cfg::R v, typename Cfg::R ref, double atol,
+                                                     double rtol, typename Cfg::C scale) {
+    using R = typename Cfg::R;
+    using C = typename Cfg::C;
+    if constexpr (Cfg::MIXED) {
+        const R tol = pymax(R(atol) + R(rtol) * R(scale) * absv(ref), R(1e-16));
+        return C(v / tol);
+    } else {
+        C tol = C(atol) + C(rtol) * scale * C(absv(ref));
+        tol = pymax(tol, C(1e-16));
+        return C(v) / tol;
+    }
+}
+
 template <class Cfg, int K>
 __device__ __forceinline__ typename Cfg::C weighted_norm2(const typename Cfg::R* v, const typename Cfg::R* ref,
                                                           typename Cfg::C scale) {
@@ -24,7 +46,8 @@ __device__ __forceinline__ typename Cfg::C weighted_norm2(const typename Cfg::R*
     C nrm2 = C(0);
 #pragma unroll
     for (int i = 0; i < K; ++i) {
-        const C ratio = C(absv(v[i])) / krylov_tol<Cfg>(i, ref[i % Cfg::N], scale);
+        const int k = i % Cfg::N;
+        const C ratio = tol_ratio<Cfg>(absv(v[i]), ref[k], Cfg::katol(k), Cfg::krtol(k), scale);
         nrm2 += ratio * ratio;
     }
     return nrm2 * (C(1) / C(K));

@@ -451,9 +451,7 @@ struct FirkProblem {
 #pragma unroll
             for (int k = 0; k < N; ++k) {
                 const R ref = pymax(absv(Y[k]), absv(base[k]));
-                C tol = C(Cfg::natol(k)) + C(Cfg::nrtol(k)) * ctx->tol_scale * C(ref);
-                tol = pymax(tol, C(1e-16));
-                const C ratio = C(delta[i * N + k]) / tol;
+                const C ratio = tol_ratio<Cfg>(delta[i * N + k], ref, Cfg::natol(k), Cfg::nrtol(k), ctx->tol_scale);
                 nrm2 += ratio * ratio;
             }
         }
@@ -639,9 +637,7 @@ struct DirkProblem {
         for (int k = 0; k < N; ++k) {
             const R sv = base[k] + a * z[k];
             const R ref = pymax(absv(sv), absv(step_start[k]));
-            C tol = C(Cfg::natol(k)) + C(Cfg::nrtol(k)) * ctx->tol_scale * C(ref);
-            tol = pymax(tol, C(1e-16));
-            const C ratio = C(delta[k]) / tol;
+            const C ratio = tol_ratio<Cfg>(delta[k], ref, Cfg::natol(k), Cfg::nrtol(k), ctx->tol_scale);
             nrm2 += ratio * ratio;
         }
         return nrm2 * (C(1) / C(K));

@@ -277,7 +277,11 @@ struct WarpDirkProblem {
         for (int k = 0; k < K; ++k) {
             if (!w.valid(k)) continue;
             const int c = w.lane + 32 * k;
-            w.m->kw[c] = R(C(1) / krylov_tol<Cfg>(c, b(k), w.tol_scale));
+            if constexpr (Cfg::MIXED)
+                w.m->kw[c] = R(1) / pymax(R(Cfg::katol(c)) + R(Cfg::krtol(c)) * R(w.tol_scale) * absv(b(k)),
+                                          R(1e-16));
+            else
+                w.m->kw[c] = R(C(1) / krylov_tol<Cfg>(c, b(k), w.tol_scale));
         }
         __syncwarp();
     }
@@ -289,9 +293,7 @@ struct WarpDirkProblem {
             const int c = w.lane + 32 * k;
             const R sv = b(k) + a * z[k];
             const R ref = pymax(absv(sv), absv(y0(k)));
-            C tol = C(Cfg::natol(c)) + C(Cfg::nrtol(c)) * w.tol_scale * C(ref);
-            tol = pymax(tol, C(1e-16));
-            const C ratio = C(delta[k]) / tol;
+            const C ratio = tol_ratio<Cfg>(delta[k], ref, Cfg::natol(c), Cfg::nrtol(c), w.tol_scale);
             nrm2 += ratio * ratio;
         }
         return warp_sum(nrm2) * (C(1) / C(Cfg::N));
