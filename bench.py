@@ -4,10 +4,10 @@
 Workload (one step): 2^20 runs of x' = y, y' = mu (1 - x^2) y - x with
 mu = 10^U[0,3], (x0, y0) ~ U[-2,2]^2 and per-run horizon t in [0, 2 mu],
 rtol = atol = 1e-6, final state saved; seed 2.  The headline path
-integrates it with ROS3P, its stage systems solved by a dense LU in
-registers (one factorisation of I - gamma h J per step, reused by the three
-stages), FP32 stepping with FP64 time, control and norms, in the persistent
-work-stealing launch.  The workload's literal solver, matrix-free GMRES, is
+integrates it with ROS3P, its stage systems solved directly in registers
+(I - gamma h J inverted in closed form once per step, reused by the three
+stages), FP32 stepping with FP64 time, step size and error-norm reduction,
+in the persistent work-stealing launch.  The workload's literal solver, matrix-free GMRES, is
 timed on the same launch and reported with its own roofline.
 
 A run counts as solved when its status word is 0 and its final state lies
@@ -380,10 +380,10 @@ def hetero_arm(args, dev):
     DP54), stiff Van der Pol (mu=10^U[0,3], x0~U[-2,2]^2; ROS3P, or Radau
     IIA5 with ``--c5-vdp radau``) and
     Robertson (k1=0.04, k2=3e7, k3=1e4 each x U[0.5,2], y0=(1,0,0); ROS3P),
-    the Rosenbrock stage systems solved by ``--linear`` (the in-register LU
-    by default); per-run rtol = 10^U[-8,-4] (a per-run scale on rtol 1e-4),
-    per-run horizon 10^U[0,3]; FP32 stepping with FP64 time, control and
-    norms; final state only; one heterogeneous persistent launch replayed as
+    the Rosenbrock stage systems solved by ``--linear`` (direct solves in
+    registers by default); per-run rtol = 10^U[-8,-4] (a per-run scale on rtol 1e-4),
+    per-run horizon 10^U[0,3]; FP32 stepping with FP64 time, step size and
+    norm reductions; final state only; one heterogeneous persistent launch replayed as
     a CUDA graph.  Runs whose rtol lies below their family's floor go to
     FP64-stepping twins of their family inside the same launch (mixed
     precision families: 1e-9, below every draw); the same launch with every
@@ -915,7 +915,7 @@ def gpu_arm(args, rank: int, world: int, dist):
             "data": "synthetic (seeded)",
             "config": {"workload": WORKLOAD, "n_systems_per_gpu": n, "algorithm": "ros3p",
                        "linear_solver": {"gmres": "gmres (unpreconditioned)",
-                                         "direct": "dense LU in registers, one factorisation per step"}.get(
+                                         "direct": "direct in registers (closed-form 2x2 inverse), one factorisation per step"}.get(
                                              args.linear, args.linear),
                        "kernel": "persistent work-stealing, runs claimed longest horizon first",
                        "precision": "mixed", "solved_if": f"status==0 and error<={SOLVED_TOL_UNITS} tol units",

@@ -18,9 +18,10 @@ multiply or divide on each element:
   update (2 K per basis vector + 7 K);
 * MR/SD iteration: preconditioner (order m applications), one application,
   two dot products (4 K), two axpys (4 K), one weighted norm;
-* direct solve (dense LU with partial pivoting): forming the operator
-  from K applications, factoring (sum over pivots of one reciprocal and
-  2 (K-k-1)^2 + (K-k-1) for the eliminations), and 2 K^2 per solve; a
+* direct solve (dense LU with partial pivoting; for K = 2 the closed-form
+  inverse): forming the operator from K applications, factoring (sum over
+  pivots of one reciprocal and 2 (K-k-1)^2 + (K-k-1) for the eliminations;
+  8 for the 2 x 2 inverse), and 2 K^2 per solve (6 for K = 2); a
   Rosenbrock step factors once and solves every stage;
 * the step-size controller: 9 N plus two powers.
 
@@ -41,6 +42,10 @@ def _f(flops: Dict[str, FlopCount], name: str) -> int:
 
 
 def direct_factor_flops(K: int, op_flops: int) -> float:
+    if K == 2:
+        # closed-form inverse: determinant (3), reciprocal (1), four scaled
+        # entries (4)
+        return K * op_flops + 8
     elim = sum(1 + 2 * (K - k - 1) ** 2 + (K - k - 1) for k in range(K))
     return K * op_flops + elim
 
@@ -48,7 +53,8 @@ def direct_factor_flops(K: int, op_flops: int) -> float:
 def linear_iteration_flops(lin: str, K: int, op_flops: int, precond_order: int, preconditioned: bool,
                            restart: int) -> float:
     if lin == "direct":
-        return 2 * K * K
+        # K = 2: two multiplies and two multiply-adds
+        return 6 if K == 2 else 2 * K * K
     if lin == "gmres":
         m = min(restart, K)
         j_avg = (m - 1) / 2.0

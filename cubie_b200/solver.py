@@ -54,7 +54,7 @@ OUTPUT_KEYS = {"output_types", "saved_state_indices", "saved_observable_indices"
                "save_variables", "summarise_variables"}
 LOOP_KEYS = {"save_every", "summarise_every", "sample_summaries_every"}
 # largest operator (states, or stages x states for fully implicit tableaus)
-# the register-resident dense LU forms
+# the register-resident direct solve forms
 DIRECT_MAX_WIDTH = 16
 EXECUTION_KEYS = {"mixed_precision", "kernel", "block_size", "min_blocks_per_sm", "max_steps", "device", "fast_math",
                   "precision", "adjoint", "layout", "schedule", "mem_proportion", "host_spill_threshold",
@@ -270,7 +270,7 @@ class Solver:
             raise ValueError("linear_correction_type must be one of 'steepest_descent', "
                              f"'minimal_residual', 'bicgstab', 'gmres', 'direct'; got '{lin}'.")
         if lin == "direct":
-            # dense LU in registers: one system per thread, small operators
+            # direct solve in registers: one system per thread, small operators
             width = n * (tab.stage_count if tab.kind == "firk" else 1)
             if self.layout != "thread":
                 raise ValueError("linear_correction_type='direct' needs layout='thread'")
