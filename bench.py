@@ -814,10 +814,15 @@ def gpu_arm(args, rank: int, world: int, dist):
         gc.enable()
     log('e2e', e2e_times)
     e2e_frac, _ = solved_fraction(res.state[-1][:, :T], res.status_codes[:T])
-    # the median step: a wall-clock step of the host API can be stretched
-    # many times over by host-side jitter outside the library (one 148 ms
-    # step among nineteen of 18 ms was seen); the mean is reported beside it
-    e2e_s, e2e_solved = aggregate(float(np.median(e2e_times)), n * e2e_frac, device=dev)
+    # the wall statistic of the reference's own benchmark protocol
+    # (benchmarks/lorenz_mean_runtime.py:44-56, 500-510): the mean of the
+    # lowest min(5, K) wall-clock steps.  Host scatter only ever adds time
+    # (on a shared host single steps were stretched from 18 ms to 60 ms and
+    # more), so the floor tracks the call's own cost; the median and the
+    # mean are reported beside it
+    k_low = min(5, len(e2e_times))
+    e2e_low = float(np.mean(np.sort(np.asarray(e2e_times))[:k_low]))
+    e2e_s, e2e_solved = aggregate(e2e_low, n * e2e_frac, device=dev)
     e2e_value = e2e_solved / e2e_s
     h2d = x0_h.numel() * 4 + mu_h.numel() * 4 + du_h.numel() * 8
     d2h = res.state.size * 4 + res.status_codes.size * 4 + 4 * 8
@@ -923,9 +928,11 @@ def gpu_arm(args, rank: int, world: int, dist):
                        "l2": "flushed (256 MB write) before every timed launch",
                        "block": new["block"]},
             "e2e": {"value": e2e_value, "unit": "systems/s", "h2d_bytes_per_step": int(h2d),
-                    "d2h_bytes_per_step": int(d2h), "ms_per_step": 1e3 * float(np.median(e2e_times)),
+                    "d2h_bytes_per_step": int(d2h), "ms_per_step": 1e3 * e2e_low,
+                    "ms_per_step_median": 1e3 * float(np.median(e2e_times)),
                     "ms_per_step_mean": 1e3 * float(np.mean(e2e_times)),
-                    "statistic": "median of the timed wall-clock steps"},
+                    "statistic": f"mean of the lowest {k_low} of {len(e2e_times)} wall-clock steps (the "
+                                 "reference benchmark's wall statistic)"},
             "gpu_launches": args.steps,
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak_fp32, "unit": "TFLOP/s",
                          "frac": achieved / peak_fp32,
