@@ -74,7 +74,9 @@ struct WarpCtx {
     C tol_scale;
     mutable R tlin;
 
-    __device__ __forceinline__ bool valid(int k) const { return lane + 32 * k < N; }
+    // every slot is a component when N is a multiple of 32 (the check then
+    // folds away from every per-lane loop)
+    __device__ __forceinline__ bool valid(int k) const { return (N % 32 == 0) || lane + 32 * k < N; }
     __device__ __forceinline__ void put(R* dst, const R* loc) const {
 #pragma unroll
         for (int k = 0; k < L; ++k)
@@ -173,7 +175,7 @@ struct WarpStageOp {
     }
     __device__ __forceinline__ C tol(int i) const {
         const int c = w.lane + 32 * i;
-        return c < Cfg::N ? C(R(1) / w.m->kw[c]) : C(1);
+        return w.valid(i) ? C(R(1) / w.m->kw[c]) : C(1);
     }
     __device__ __forceinline__ C wnorm2(const R* v) const {
         R s2 = R(0);
@@ -601,7 +603,7 @@ __device__ __forceinline__ void warp_update_summaries(WarpLane<Cfg>& L, WarpCtx<
 #pragma unroll
     for (int kk = 0; kk < WarpLane<Cfg>::SK; ++kk) {
         const int sv = w.lane + 32 * kk;
-        if (sv < Cfg::N_SUMM_STATES)
+        if (Cfg::N_SUMM_STATES % 32 == 0 || sv < Cfg::N_SUMM_STATES)
             Summ::update(w.m->ys[Cfg::Idx::summ_state(sv)], L.sbuf + kk * Summ::BUF, L.update_idx);
     }
     __syncwarp();
@@ -618,7 +620,7 @@ __device__ __forceinline__ void warp_save_summaries(WarpLane<Cfg>& L, WarpCtx<Cf
 #pragma unroll
     for (int kk = 0; kk < WarpLane<Cfg>::SK; ++kk) {
         const int sv = w.lane + 32 * kk;
-        if (sv < Cfg::N_SUMM_STATES) {
+        if (Cfg::N_SUMM_STATES % 32 == 0 || sv < Cfg::N_SUMM_STATES) {
             Summ::save(L.sbuf + kk * Summ::BUF, vals, Cfg::SAMPLES_PER_SUMMARY);
             if (in_range) {
                 R* out = static_cast<R*>(a.state_sum_out) +
