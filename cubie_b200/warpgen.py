@@ -141,6 +141,9 @@ def _emit_classes(name: str, classes: List[ExprClass], with_v: bool, tables: Lis
         for s in slot_syms:
             sym_map[s] = f"s_{s.name[1:]}"
         lines.append(f"        // class {ci}: {nm} member(s)")
+        # kept as a loop: unrolled over a lane's members the class code
+        # grew the kernel until instruction fetch bounded it
+        lines.append("        #pragma unroll 1")
         lines.append(f"        for (int m = lane; m < {nm}; m += 32) {{")
         # output index
         aff = _affine(c.members)
@@ -214,6 +217,7 @@ def _emit_cached_jacobian(classes: List[ExprClass], tables: List[str]):
         printer = _CudaPrinter(sym_map)
         out_idx = _index_expr("fj", ci, 99, c.members, tables)
         head = [f"        // class {ci}: {nm} member(s), {len(v_syms)} coefficient(s) each",
+                "        #pragma unroll 1",
                 f"        for (int m = lane; m < {nm}; m += 32) {{", f"            const int o = {out_idx};"]
         fj += head
         jm += head
