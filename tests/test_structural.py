@@ -205,3 +205,18 @@ def test_torn_dae_solution_gpu(cuda_device, algorithm):
     bar = 2e-3 if algorithm == "backwards_euler" else 1e-6
     assert abs(x - x_ref) < bar and abs(z - _z_of_x(x_ref)) < bar
     assert abs(z**5 + z - x) < 1e-5
+
+
+def test_structural_helpers():
+    """The matching, component ordering and alias detection on small
+    hand-made cases."""
+    from cubie_b200.structural import _alias, _components, _match
+    x, y, z = _s("x"), _s("y"), _s("z")
+    assert _alias(x - y, {x, y}) in ((x, y, 1), (y, x, 1))
+    assert _alias(x + y, {x, y})[2] == -1
+    assert _alias(2 * x - y, {x, y}) is None and _alias(x - y + 1, {x, y}) is None
+    # equations {x, y}, {y}, {y, z}: the only complete matching is x, y, z
+    assert _match([{x, y}, {y}, {y, z}], [x, y, z]) == [0, 1, 2]
+    assert _match([{x}, {x}], [x, y]) is None
+    # 0 -> 1 -> 2 -> 1: components {1, 2} before {0}
+    assert _components(3, [[1], [2], [1]]) == [[1, 2], [0]]
