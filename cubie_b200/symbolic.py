@@ -501,13 +501,15 @@ def _create_dae_system(eqs, precision, state_defaults, obs_names, param_defaults
             if target not in unknowns:
                 raise ValueError(f"'{lhs}' differentiates '{target}', which is not a declared state")
             if m2:
-                # companion state for the first derivative (x_t, x_tt ...)
+                # companion state for the first derivative: x_t (a declared
+                # state of that name is used as it, with its initial value)
                 comp = f"{target}_t"
-                while comp in unknowns or comp in inputs or comp in symbols:
-                    comp += "_"
-                unknowns[comp] = symbols.setdefault(comp, sp.Symbol(comp, real=True))
-                order.insert(order.index(target) + 1, comp)
-                defaults.setdefault(comp, 0.0)
+                if comp not in unknowns:
+                    while comp in inputs or comp in symbols:
+                        comp += "_"
+                    unknowns[comp] = symbols.setdefault(comp, sp.Symbol(comp, real=True))
+                    order.insert(order.index(target) + 1, comp)
+                    defaults.setdefault(comp, 0.0)
                 set_derivative(target, unknowns[comp])
                 set_derivative(comp, expr)
             else:

@@ -80,6 +80,9 @@ def test_linear_block_solved_analytically_and_second_derivative_lowered():
     osc = create_ODE_system(["d(d(x, t), t) = -x"], states={"x": 1.0})
     assert osc.state_names == ["x", "x_t"] and osc.mass is None
     assert _deriv(osc, "x") == _s("x_t") and sp.simplify(_deriv(osc, "x_t") + x) == 0
+    # a declared companion keeps its initial value
+    osc2 = create_ODE_system(["d(d(x, t), t) = -x"], states={"x": 1.0, "x_t": 0.5})
+    assert osc2.state_names == ["x", "x_t"] and osc2.initial_values["x_t"] == 0.5
 
 
 def test_two_torn_residuals_pair_with_their_unknowns():
