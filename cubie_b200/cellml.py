@@ -27,9 +27,11 @@ component-level and user-defined base units).  A model variable is held in
 the units of its defining occurrence; an occurrence in another component
 with compatible but different units reads it scaled by the ratio of the
 factors, and equations defining it there are scaled back (the reference
-converts through pint, cellmlmanip's units handling).  Incompatible units
-across a connection raise ``ValueError``; units with an offset (celsius)
-raise ``NotImplementedError``.
+converts through pint, cellmlmanip's units handling).  Units with an
+offset (celsius, or a CellML 1.x unit with an ``offset`` attribute) convert
+affinely, x_occ = k x_src + b; in products of units an offset describes a
+difference and drops out.  Incompatible units across a connection raise
+``ValueError``.
 
 Imports (CellML 1.1 and 2.0): components and units of other documents,
 found relative to the importing file; an imported component brings the
@@ -215,8 +217,10 @@ _BUILTIN_UNITS = {
     "liter": _u(1e-3, m=3), "litre": _u(1e-3, m=3), "lumen": _u(cd=1), "lux": _u(m=-2, cd=1),
     "newton": _u(m=1, kg=1, s=-2), "ohm": _u(m=2, kg=1, s=-3, A=-2), "pascal": _u(m=-1, kg=1, s=-2),
     "siemens": _u(m=-2, kg=-1, s=3, A=2), "tesla": _u(kg=1, s=-2, A=-1), "volt": _u(m=2, kg=1, s=-3, A=-1),
-    "watt": _u(m=2, kg=1, s=-3), "weber": _u(m=2, kg=1, s=-2, A=-1),
+    "watt": _u(m=2, kg=1, s=-3), "weber": _u(m=2, kg=1, s=-2, A=-1), "celsius": _u(K=1),
 }
+# additive offsets to the base units (value_base = factor * value + offset)
+_BUILTIN_OFFSET = {"celsius": 273.15}
 
 
 class _Units:
@@ -240,8 +244,6 @@ class _Units:
             return self._cache[name]
         scope = self._find(name)
         if scope is None:
-            if name == "celsius":
-                raise NotImplementedError("units with an offset (celsius) are not converted")
             if name not in _BUILTIN_UNITS:
                 raise ValueError(f"unknown units '{name}'")
             return _BUILTIN_UNITS[name]
@@ -252,9 +254,13 @@ class _Units:
             out = (1.0, {name: 1.0})
         else:
             factor, dims = 1.0, {}
-            for un in el.findall(scope.cml + "unit"):
-                if float(un.get("offset", "0") or 0) != 0.0:
-                    raise NotImplementedError(f"units '{name}': units with an offset are not converted")
+            children = el.findall(scope.cml + "unit")
+            for un in children:
+                if float(un.get("offset", "0") or 0) != 0.0 and (
+                        len(children) != 1 or float(un.get("exponent", "1")) != 1.0):
+                    # CellML 1.x allows an offset only on a sole unit of
+                    # exponent 1
+                    raise ValueError(f"units '{name}': an offset needs a single unit of exponent 1")
                 f, d = scope.resolve(un.get("units"), _depth + 1)
                 pre = un.get("prefix", "0")
                 pexp = _PREFIX[pre] if pre in _PREFIX else int(pre)
@@ -266,6 +272,30 @@ class _Units:
             out = (factor, {k: v for k, v in dims.items() if abs(v) > 1e-12})
         self._cache[name] = out
         return out
+
+    def offset(self, name: str, _depth: int = 0) -> float:
+        """The additive offset of ``name`` to its base units
+        (value_base = factor * value + offset): 273.15 for celsius; for a
+        unit defined as one unit of exponent 1 with multiplier m, prefix p
+        and offset o over a unit of factor f_r and offset o_r,
+        f_r * o + o_r (CellML 1.1 section 5.2.2: the offset is added after
+        the multiplier and prefix); zero for products of units, whose
+        offsets describe differences."""
+        scope = self._find(name)
+        if scope is None:
+            return _BUILTIN_OFFSET.get(name, 0.0)
+        if _depth > 64:
+            raise ValueError(f"units '{name}' are defined in terms of themselves")
+        el = scope.defs[name]
+        if el.get("base_units") == "yes":
+            return 0.0
+        children = el.findall(scope.cml + "unit")
+        if len(children) != 1 or float(children[0].get("exponent", "1")) != 1.0:
+            return 0.0
+        un = children[0]
+        f_r, _ = scope.resolve(un.get("units"), _depth + 1)
+        o_r = scope.offset(un.get("units"), _depth + 1)
+        return f_r * float(un.get("offset", "0") or 0) + o_r
 
 
 def _scale(factor: float) -> sp.Expr:
@@ -490,10 +520,25 @@ def load_cellml_model(path, precision=np.float32, name: Optional[str] = None,
                              f"'{sources[root_][0]}' with incompatible units")
         return f_src / f_occ
 
+    def b(c, v):
+        """Additive part of the conversion from the source's units to this
+        occurrence's: x_occ = k x_src + (o_src - o_occ) / f_occ."""
+        root_ = uf.find((c, v))
+        sc, sv = sources[root_]
+        if (sc, sv) == (c, v):
+            return 0.0
+        o_src = comp_els[sc][1].offset(comps[sc][sv]["units"] or "dimensionless")
+        o_occ = comp_els[c][1].offset(comps[c][v]["units"] or "dimensionless")
+        if o_src == o_occ:
+            return 0.0
+        f_occ, _ = unit_of(c, v)
+        return (o_src - o_occ) / f_occ
+
     def read(c, local):
-        kk = k(c, local)
+        kk, bb = k(c, local), b(c, local)
         sym = symbols[uf.find((c, local))]
-        return sym if kk == 1.0 else _scale(kk) * sym
+        out = sym if kk == 1.0 else _scale(kk) * sym
+        return out if bb == 0.0 else out + _scale(bb)
 
     derivatives: Dict[str, sp.Expr] = {}
     assignments: List[Tuple[sp.Symbol, sp.Expr]] = []
@@ -503,9 +548,14 @@ def load_cellml_model(path, precision=np.float32, name: Optional[str] = None,
         conv = _MathML(lambda local, c=cname: read(c, local))
         expr = conv.convert(rhs)
         root_ = uf.find((cname, target))
-        # d(k_x x)/d(k_t t) = rhs  ->  dx/dt = (k_t / k_x) rhs;  k_x x = rhs  ->  x = rhs / k_x
+        # d(k_x x + b_x)/d(k_t t) = rhs  ->  dx/dt = (k_t / k_x) rhs;
+        # k_x x + b_x = rhs  ->  x = (rhs - b_x) / k_x
         kx = k(cname, target)
         kt = k(cname, tname) if kind == "ode" else 1.0
+        if kind != "ode":
+            bx = b(cname, target)
+            if bx != 0.0:
+                expr = expr - _scale(bx)
         if kt / kx != 1.0:
             expr = _scale(kt / kx) * expr
         if kind == "ode":

@@ -345,3 +345,83 @@ def test_cellml_import_brings_the_encapsulated_components(tmp_path):
     _write(tmp_path, cyc, "lib.cellml")
     with pytest.raises(ValueError, match="cycle"):
         load_cellml_model(tmp_path / "main.cellml")
+
+
+TEMP_CELLML_11 = """<?xml version="1.0"?>
+<model xmlns="http://www.cellml.org/cellml/1.1#" xmlns:cellml="http://www.cellml.org/cellml/1.1#" name="temp">
+  <units name="per_second"><unit units="second" exponent="-1"/></units>
+  <units name="fahrenheit"><unit units="kelvin" multiplier="0.5555555555555556" offset="255.37222222222223"/></units>
+  <component name="env">
+    <variable name="time" units="second" public_interface="out"/>
+  </component>
+  <component name="body">
+    <variable name="time" units="second" public_interface="in"/>
+    <variable name="T" units="kelvin" initial_value="310" public_interface="out"/>
+    <variable name="Ta" units="celsius" public_interface="in"/>
+    <variable name="k" units="per_second" initial_value="0.1"/>
+    <math xmlns="http://www.w3.org/1998/Math/MathML">
+      <apply><eq/><apply><diff/><bvar><ci>time</ci></bvar><ci>T</ci></apply>
+        <apply><times/><ci>k</ci><apply><minus/><apply><plus/><ci>Ta</ci>
+          <cn cellml:units="kelvin">273.15</cn></apply><ci>T</ci></apply></apply></apply>
+    </math>
+  </component>
+  <component name="room">
+    <variable name="Ta" units="celsius" initial_value="20" public_interface="out"/>
+  </component>
+  <component name="probe">
+    <variable name="T" units="celsius" public_interface="in"/>
+    <variable name="Tc" units="celsius"/>
+    <variable name="Tf" units="fahrenheit" public_interface="out"/>
+    <math xmlns="http://www.w3.org/1998/Math/MathML">
+      <apply><eq/><ci>Tc</ci><ci>T</ci></apply>
+      <apply><eq/><ci>Tf</ci><ci>T</ci></apply>
+    </math>
+  </component>
+  <component name="reader">
+    <variable name="Tf" units="kelvin" public_interface="in"/>
+    <variable name="Tk" units="kelvin"/>
+    <math xmlns="http://www.w3.org/1998/Math/MathML">
+      <apply><eq/><ci>Tk</ci><ci>Tf</ci></apply>
+    </math>
+  </component>
+  <connection><map_components component_1="env" component_2="body"/>
+    <map_variables variable_1="time" variable_2="time"/></connection>
+  <connection><map_components component_1="room" component_2="body"/>
+    <map_variables variable_1="Ta" variable_2="Ta"/></connection>
+  <connection><map_components component_1="body" component_2="probe"/>
+    <map_variables variable_1="T" variable_2="T"/></connection>
+  <connection><map_components component_1="probe" component_2="reader"/>
+    <map_variables variable_1="Tf" variable_2="Tf"/></connection>
+</model>
+"""
+
+
+def test_cellml_offset_units_convert_affinely(tmp_path):
+    """A temperature held in kelvin and read in celsius elsewhere shifts by
+    273.15; a CellML 1.1 unit with an offset (Fahrenheit over kelvin)
+    converts through its multiplier and offset when read across a
+    connection; the ODE in kelvin is unchanged by the offsets of the other
+    occurrences."""
+    from cubie_b200.cellml import load_cellml_model
+    ode = load_cellml_model(_write(tmp_path, TEMP_CELLML_11, "temp.cellml"), precision=np.float64,
+                            observables=["Tc", "Tf", "Tk"])
+    T = sp.Symbol("T", real=True)
+    assert ode.state_names == ["T"] and ode.initial_values["T"] == 310.0
+    asg = dict((str(a), e) for a, e in ode.assignments)
+    # dT/dt = k ((Ta_C + 273.15) - T) with the room at 20 C
+    dT = ode.derivatives["T"].subs({sp.Symbol("k", real=True): 0.1, sp.Symbol("Ta", real=True): 20.0})
+    assert abs(float(dT.subs(T, 300.0)) - 0.1 * (293.15 - 300.0)) < 1e-12
+    # probe: T (kelvin) read in celsius
+    assert abs(float(asg["Tc"].subs(T, 310.0)) - 36.85) < 1e-12
+    # within a component an equation relates values in their own units
+    # (no conversion): Tf holds the probe's celsius number as fahrenheit
+    assert abs(float(asg["Tf"].subs(T, 310.0)) - 36.85) < 1e-12
+    # the reader sees Tf in kelvin: 36.85 F = 36.85 * 5/9 + 255.372 K
+    tk = asg["Tk"].subs(sp.Symbol("Tf", real=True), asg["Tf"]).subs(T, 310.0)
+    assert abs(float(tk) - (36.85 * 0.5555555555555556 + 255.37222222222223)) < 1e-9
+    # an offset on a compound unit is rejected
+    bad = TEMP_CELLML_11.replace('<units name="fahrenheit"><unit units="kelvin" multiplier="0.5555555555555556" '
+                                 'offset="255.37222222222223"/></units>',
+                                 '<units name="fahrenheit"><unit units="kelvin" exponent="2" offset="1"/></units>')
+    with pytest.raises(ValueError, match="offset"):
+        load_cellml_model(_write(tmp_path, bad, "bad_temp.cellml"), observables=["Tc", "Tf", "Tk"])
