@@ -39,10 +39,13 @@ components it encapsulates (named ``<local name>__<name>``) and the
 connections among them; imports may nest.  Both documents use the same
 CellML version.
 
-Not done here: ``reset`` elements (rejected with ``NotImplementedError``),
-and the reference's optional rewrite of removable
-Goldman-Hodgkin-Katz singularities (``U / (exp(U) - 1)`` is compiled as
-written; it is finite everywhere except exactly at ``U = 0``).
+Removable Goldman-Hodgkin-Katz singularities (``N / (exp(U) - 1)`` with U
+affine in the membrane voltage and N vanishing at U = 0) are rewritten as
+(N / U) times U / (exp(U) - 1), the latter from its Taylor series near
+U = 0, when ``fix_singularities`` is set (the reference's default, which
+bridges the singular point by linear interpolation instead).
+
+Not done here: ``reset`` elements (rejected with ``NotImplementedError``).
 
 States are the variables that have a ``diff`` equation; variables with an
 initial value and no equation are constants unless named in
@@ -55,6 +58,7 @@ share a name.
 from __future__ import annotations
 
 import hashlib
+import warnings
 import re
 import xml.etree.ElementTree as ET
 from pathlib import Path
@@ -406,9 +410,13 @@ def load_cellml_model(path, precision=np.float32, name: Optional[str] = None,
     """Read a CellML file into a :class:`SymbolicODE` (arguments as the
     reference's ``load_cellml_model``).  ``parameters`` and ``observables``
     name model variables (by their model name, or ``component__name``).
-    ``fix_singularities`` and ``voltage_variable`` are accepted for the same
-    call signature; no rewrite is applied (see the module notes).  The
-    constants editor GUI (``show_gui``) is not part of this engine."""
+    With ``fix_singularities`` (the default) removable
+    Goldman-Hodgkin-Katz singularities in the membrane voltage
+    (``voltage_variable``, or the state auto-detected as the reference
+    detects it: a V or voltage variable of a membrane component, with a
+    warning and no rewrite when none is found) are rewritten to a form that
+    is finite at the singular point.  The constants editor GUI
+    (``show_gui``) is not part of this engine."""
     if not isinstance(path, (str, Path)):
         raise TypeError("path must be a string or a Path")
     path = Path(path)
@@ -593,6 +601,27 @@ def load_cellml_model(path, precision=np.float32, name: Optional[str] = None,
     for o in obs_list:
         if o not in alg_names:
             raise ValueError(f"observable '{o}' is not defined by an algebraic equation")
+    if fix_singularities:
+        vname = voltage_variable
+        if vname is None:
+            # a state of a component named like "membrane" whose variable
+            # is V or a voltage (as the reference detects it)
+            for root_ in state_roots:
+                comp_name, var_name = sources[root_]
+                low = var_name.lower()
+                if "membrane" in comp_name.lower() and (low == "v" or "voltage" in low):
+                    vname = names[root_]
+                    break
+            if vname is None:
+                warnings.warn("fix_singularities is enabled but no membrane voltage state could be "
+                              "auto-detected; skipping singularity removal. Pass voltage_variable to apply it.",
+                              UserWarning, stacklevel=2)
+        elif vname not in states and vname not in {a.name for a, _ in assignments}:
+            raise ValueError(f"Could not resolve membrane voltage variable {vname!r} for singularity removal.")
+        if vname is not None:
+            Vsym = sp.Symbol(vname, real=True)
+            derivatives = {k: _remove_ghk_singularities(e, Vsym) for k, e in derivatives.items()}
+            assignments = [(a, _remove_ghk_singularities(e, Vsym)) for a, e in assignments]
     base = set(states) | set(params) | set(consts) | {"t"}
     assignments = _topological(assignments, base)
     # derivative assignments go last, in state order, as the string front end builds them
@@ -603,6 +632,70 @@ def load_cellml_model(path, precision=np.float32, name: Optional[str] = None,
                        name=name or path.stem,
                        source="cellml:" + hashlib.sha256(_model_bytes(path)).hexdigest() + "|P" + ",".join(params)
                        + "|O" + ",".join(obs_list))
+
+
+# --------------------------------------------------------------------------
+# removable Goldman-Hodgkin-Katz singularities: N(V) / (exp(U(V)) - 1) with
+# U affine in the membrane voltage V and N vanishing where U does is finite
+# at U = 0 but evaluates to 0 / 0 there.  It is rewritten as
+# (N / U) * B(U), B(U) = U / (exp(U) - 1), with B taken from its Taylor
+# series 1 - U/2 + U^2/12 - U^4/720 for |U| < 1e-2 (truncation error below
+# 1e-14 relative; the direct form loses about eps / |U| there to the
+# cancellation in exp(U) - 1).
+# --------------------------------------------------------------------------
+_GHK_SERIES_BOUND = 1e-2
+
+
+def _bernoulli_factor(U: sp.Expr) -> sp.Expr:
+    series = 1 - U / 2 + U ** 2 / 12 - U ** 4 / 720
+    return sp.Piecewise((series, sp.Abs(U) < _GHK_SERIES_BOUND), (U / (sp.exp(U) - 1), True))
+
+
+def _exp_minus_one(D: sp.Expr):
+    """(c, U) with D = c (exp(U) - 1), or None."""
+    D = sp.expand(D, power_exp=False, power_base=False, log=False)
+    terms = sp.Add.make_args(D)
+    if len(terms) != 2:
+        return None
+    exps = [t for t in terms if t.func is sp.exp or (t.is_Mul and any(f.func is sp.exp for f in t.args))]
+    rest = [t for t in terms if t not in exps]
+    if len(exps) != 1 or len(rest) != 1 or not rest[0].is_number:
+        return None
+    coeff, ex = exps[0].as_coeff_Mul()
+    if ex.func is not sp.exp or rest[0] != -coeff:
+        return None
+    return coeff, ex.args[0]
+
+
+def _remove_ghk_singularities(expr: sp.Expr, V: sp.Symbol) -> sp.Expr:
+    def visit(e):
+        if not e.args:
+            return e
+        e = e.func(*[visit(a) for a in e.args])
+        if not e.is_Mul:
+            return e
+        for k, factor in enumerate(e.args):
+            if not (factor.is_Pow and factor.exp == -1):
+                continue
+            found = _exp_minus_one(factor.base)
+            if found is None:
+                continue
+            c, U = found
+            try:
+                poly = sp.Poly(U, V)
+            except sp.PolynomialError:
+                continue
+            if poly.degree() != 1:
+                continue
+            V0 = sp.solve(U, V)
+            if len(V0) != 1:
+                continue
+            num = sp.Mul(*[f for j, f in enumerate(e.args) if j != k])
+            if sp.simplify(num.subs(V, V0[0])) != 0:
+                continue
+            return sp.cancel(num / U) / c * _bernoulli_factor(U)
+        return e
+    return visit(expr)
 
 
 def _model_bytes(path: Path) -> bytes:

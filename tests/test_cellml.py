@@ -425,3 +425,68 @@ def test_cellml_offset_units_convert_affinely(tmp_path):
                                  '<units name="fahrenheit"><unit units="kelvin" exponent="2" offset="1"/></units>')
     with pytest.raises(ValueError, match="offset"):
         load_cellml_model(_write(tmp_path, bad, "bad_temp.cellml"), observables=["Tc", "Tf", "Tk"])
+
+
+GHK_CELLML_10 = """<?xml version="1.0"?>
+<model xmlns="http://www.cellml.org/cellml/1.0#" xmlns:cellml="http://www.cellml.org/cellml/1.0#" name="ghk">
+  <units name="ms"><unit units="second" prefix="milli"/></units>
+  <units name="mV"><unit units="volt" prefix="milli"/></units>
+  <units name="per_ms"><unit units="second" prefix="milli" exponent="-1"/></units>
+  <units name="mV_per_ms"><unit units="mV"/><unit units="ms" exponent="-1"/></units>
+  <component name="environment">
+    <variable name="time" units="ms" public_interface="out"/>
+  </component>
+  <component name="membrane">
+    <variable name="time" units="ms" public_interface="in"/>
+    <variable name="V" units="mV" initial_value="-65" public_interface="out"/>
+    <variable name="m" units="dimensionless" initial_value="0.05"/>
+    <variable name="alpha_m" units="per_ms"/>
+    <math xmlns="http://www.w3.org/1998/Math/MathML">
+      <apply><eq/><ci>alpha_m</ci>
+        <apply><divide/>
+          <apply><times/><cn cellml:units="per_ms">0.1</cn>
+            <apply><plus/><ci>V</ci><cn cellml:units="mV">40</cn></apply></apply>
+          <apply><minus/><cn cellml:units="dimensionless">1</cn>
+            <apply><exp/><apply><divide/>
+              <apply><minus/><apply><plus/><ci>V</ci><cn cellml:units="mV">40</cn></apply></apply>
+              <cn cellml:units="mV">10</cn></apply></apply></apply></apply></apply>
+      <apply><eq/><apply><diff/><bvar><ci>time</ci></bvar><ci>m</ci></apply>
+        <apply><times/><ci>alpha_m</ci><apply><minus/><cn cellml:units="dimensionless">1</cn><ci>m</ci></apply></apply></apply>
+      <apply><eq/><apply><diff/><bvar><ci>time</ci></bvar><ci>V</ci></apply>
+        <apply><minus/><ci>m</ci></apply></apply>
+    </math>
+  </component>
+  <connection><map_components component_1="environment" component_2="membrane"/>
+    <map_variables variable_1="time" variable_2="time"/></connection>
+</model>
+"""
+
+
+def test_cellml_removable_ghk_singularity_is_rewritten(tmp_path):
+    """alpha_m = 0.1 (V + 40) / (1 - exp(-(V + 40) / 10)) is 0 / 0 at
+    V = -40 as written; with the membrane voltage detected, the rewritten
+    rate is finite there (its limit, 1) and equal to the original away from
+    it; with fix_singularities=False the expression is kept as written."""
+    from cubie_b200.cellml import load_cellml_model
+    path = _write(tmp_path, GHK_CELLML_10, "ghk.cellml")
+    V = sp.Symbol("V", real=True)
+    fixed = load_cellml_model(path, precision=np.float64, observables=["alpha_m"])
+    raw = load_cellml_model(path, precision=np.float64, observables=["alpha_m"], fix_singularities=False)
+    a_fixed = dict((str(a), e) for a, e in fixed.assignments)["alpha_m"]
+    a_raw = dict((str(a), e) for a, e in raw.assignments)["alpha_m"]
+    f_fixed = sp.lambdify(V, a_fixed, "math")
+    f_raw = sp.lambdify(V, a_raw, "math")
+    assert abs(f_fixed(-40.0) - 1.0) < 1e-15
+    with pytest.raises(ZeroDivisionError):
+        f_raw(-40.0)
+    # against the written rate evaluated in 50-digit arithmetic (in FP64
+    # the written form itself loses about eps / |U| near the singularity;
+    # closer than about 1e-4 the rounding of its decimal constants, which
+    # moves the numerator's zero by ~1e-15, decides the written value)
+    for v in (-40.0 - 3e-4, -40.0 + 2e-3, -40.5, -65.0, 10.0):
+        exact = float(a_raw.subs(V, sp.Float(repr(v), 50)).evalf(50))
+        assert abs(f_fixed(v) - exact) <= 1e-10 * abs(exact), v
+    assert abs(f_fixed(-40.0 + 1e-9) - (1.0 + 5e-11)) < 1e-14      # the limit's first-order term
+    # an explicitly named voltage that does not exist is an error
+    with pytest.raises(ValueError, match="membrane voltage"):
+        load_cellml_model(path, voltage_variable="U")
