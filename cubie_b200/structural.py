@@ -23,8 +23,14 @@ systems, in SymPy on the host, before code generation:
   elimination or tearing and stay as states);
 * the remaining implicit equations are matched to the remaining algebraic
   unknowns (every equation to a distinct unknown it contains); more
-  equations than unknowns, fewer, or no complete matching (a structurally
-  singular, higher-index system) raise;
+  equations than unknowns, or fewer, raise;
+* a set of constraints that cannot be matched (a higher-index system, such
+  as the pendulum in Cartesian coordinates) is differentiated along the
+  differential equations until its highest derivatives match
+  (Pantelides' criterion); the lower derivatives stay as invariants, and
+  each demotes one differential state it contains to an algebraic unknown
+  (the lowest ``state_priority`` first), as the dummy-derivative method
+  selects states (see ``_reduce_index``);
 * the matched blocks are visited in dependency order (strongly connected
   components of the equation graph): a single equation affine in its
   unknown, or a block linear in its unknowns with a nonsingular matrix, is
@@ -35,10 +41,11 @@ The result carries the differential states, the algebraic states with one
 residual each, and the observed definitions.  The system it becomes has
 the states in that order and the mass matrix diag(1, ..., 1, 0, ..., 0):
 ``M y' = F(y)`` with F the derivatives of the differential states followed
-by the residuals.  Index reduction of higher-index systems (Pantelides'
-algorithm and dummy derivatives, ``pantelides.py``,
-``dummy_derivatives.py``) is not built: such input is reported as
-structurally singular.
+by the residuals.  The state selection of the index reduction is static,
+as the reference's priorities make it: it holds while the invariants stay
+regular in the demoted states along the solution (the pendulum with y and
+vy kept needs x away from 0).  Constraints whose derivatives involve the
+derivatives of algebraic unknowns are not reduced (they raise).
 """
 
 from __future__ import annotations
@@ -191,10 +198,114 @@ def _solve_linear(gs: Sequence[sp.Expr], zs: Sequence[sp.Symbol]) -> Optional[Di
     return {z: sp.simplify(sol[k]) for k, z in enumerate(zs)}
 
 
+def _time_derivative(g: sp.Expr, derivs: Mapping[sp.Symbol, sp.Expr], algebraic: Set[sp.Symbol],
+                     time: sp.Symbol) -> sp.Expr:
+    """dg/dt along the solution: the explicit time dependence plus
+    sum_u dg/du f_u over the differential unknowns.  A constraint whose
+    derivative would need an algebraic unknown's derivative is outside this
+    scheme (None)."""
+    out = sp.diff(g, time)
+    for u in g.free_symbols:
+        if u in derivs:
+            out += sp.diff(g, u) * derivs[u]
+        elif u in algebraic and sp.diff(g, u) != 0:
+            return None
+    return out
+
+
+def _reduce_index(residuals: List[sp.Expr], derivs: Dict[sp.Symbol, sp.Expr], algebraic: List[sp.Symbol],
+                  prio: Mapping[sp.Symbol, float], order: Mapping[sp.Symbol, int], keep_always: Set[sp.Symbol],
+                  time: sp.Symbol):
+    """Index reduction of a semi-explicit DAE whose constraints do not
+    determine its algebraic unknowns (Pantelides' criterion on the
+    equation/unknown graph, Pantelides 1988, with the constraint chains of
+    Mattsson and Soederlind's dummy-derivative method, 1993).
+
+    Every implicit equation in a set that an augmenting path cannot match
+    to distinct algebraic unknowns is replaced by its time derivative along
+    the differential equations, until the highest derivatives match; the
+    lower members of each chain stay as invariants.  Each invariant then
+    demotes one differential state that it contains to an algebraic
+    unknown, dropping that state's differential equation (its derivative
+    is implied by the chain), with the lowest ``state_priority`` demoted
+    first and irreducible states kept.  The selection is static: it holds
+    while the invariants' Jacobian in the demoted states stays regular
+    along the solution, as with the reference's priorities.  Returns the
+    residuals (highest derivatives, then invariants) and the algebraic
+    unknowns (the originals, then the demoted states)."""
+    chains = [[g] for g in residuals]
+    alg_set = set(algebraic)
+    for _ in range(8):
+        top = [c[-1] for c in chains]
+        inc = [set(g.free_symbols) & alg_set for g in top]
+        owner: Dict[sp.Symbol, int] = {}
+        failed = None
+        for e in range(len(top)):
+            seen_v: Set[sp.Symbol] = set()
+            seen_e: Set[int] = set()
+
+            def augment(i):
+                seen_e.add(i)
+                for v in sorted(inc[i], key=lambda z: order[z]):
+                    if v in seen_v:
+                        continue
+                    seen_v.add(v)
+                    if v not in owner or augment(owner[v]):
+                        owner[v] = i
+                        return True
+                return False
+
+            if not augment(e):
+                failed = seen_e
+                break
+        if failed is None:
+            break
+        for e in failed:
+            d = _time_derivative(chains[e][-1], derivs, alg_set, time)
+            if d is None:
+                raise InvalidSystemError("a constraint's derivative needs the derivative of an algebraic unknown; "
+                                         "this index reduction differentiates constraints on the differential "
+                                         "states only")
+            if d == 0:
+                raise InvalidSystemError("a constraint's time derivative vanishes identically (a redundant "
+                                         "or inconsistent system)")
+            chains[e].append(d)
+    else:
+        raise InvalidSystemError("index reduction did not reach an index-1 system in 8 differentiations")
+    invariants = [g for c in chains for g in c[:-1]]
+    diff_states = [u for u in order if u in derivs]
+    # demote the least preferred states first: lowest priority, then the
+    # later declared
+    ranked = sorted((u for u in diff_states if u not in keep_always), key=lambda u: (prio.get(u, 0.0), -order[u]))
+    inc = [[u for u in ranked if u in g.free_symbols] for g in invariants]
+    owner2: Dict[sp.Symbol, int] = {}
+
+    def augment2(i, seen):
+        for v in inc[i]:
+            if v in seen:
+                continue
+            seen.add(v)
+            if v not in owner2 or augment2(owner2[v], seen):
+                owner2[v] = i
+                return True
+        return False
+
+    for i in range(len(invariants)):
+        if not augment2(i, set()):
+            raise InvalidSystemError("no state selection satisfies the invariants of the reduced system")
+    demoted = sorted(owner2, key=lambda u: order[u])
+    for u in demoted:
+        derivs.pop(u)
+    by_state = {u: invariants[i] for u, i in owner2.items()}
+    new_res = [c[-1] for c in chains] + [by_state[u] for u in demoted]
+    return new_res, list(algebraic) + demoted
+
+
 def structural_simplify(unknowns: Sequence[sp.Symbol], derivatives: Mapping[sp.Symbol, sp.Expr],
                         implicit: Sequence[sp.Expr], explicit: Sequence[Tuple[sp.Symbol, sp.Expr]] = (),
                         state_priority: Optional[Mapping[sp.Symbol, float]] = None,
-                        irreducible: Iterable[sp.Symbol] = (), inline_linear_sccs: bool = True) -> SimplifiedSystem:
+                        irreducible: Iterable[sp.Symbol] = (), inline_linear_sccs: bool = True,
+                        time: Optional[sp.Symbol] = None) -> SimplifiedSystem:
     """Index-1 structural simplification (see the module docstring).
 
     ``unknowns``: the declared states, in order; ``derivatives``: the
@@ -204,6 +315,7 @@ def structural_simplify(unknowns: Sequence[sp.Symbol], derivatives: Mapping[sp.S
     symbol (parameters, constants, drivers, t)."""
     order = {u: k for k, u in enumerate(unknowns)}
     prio = dict(state_priority or {})
+    time = time if time is not None else sp.Symbol("t", real=True)
     keep_always = set(irreducible)
     derivs: Dict[sp.Symbol, sp.Expr] = dict(derivatives)
     residuals: List[sp.Expr] = list(implicit)
@@ -288,9 +400,11 @@ def structural_simplify(unknowns: Sequence[sp.Symbol], derivatives: Mapping[sp.S
     incidence = [set(g.free_symbols) & set(algebraic) for g in residuals]
     matched = _match(incidence, algebraic)
     if matched is None:
-        raise InvalidSystemError(
-            "the implicit equations are structurally singular in the algebraic unknowns (a higher-index "
-            "system); index reduction is not built")
+        residuals, algebraic = _reduce_index(residuals, derivs, algebraic, prio, order, keep_always, time)
+        incidence = [set(g.free_symbols) & set(algebraic) for g in residuals]
+        matched = _match(incidence, algebraic)
+        if matched is None:
+            raise InvalidSystemError("the implicit equations stay structurally singular after index reduction")
     var_of = {e: algebraic[v] for e, v in enumerate(matched)}
     eq_of = {z: e for e, z in var_of.items()}
     # equation e depends on equation f when e contains f's unknown

@@ -100,12 +100,10 @@ def test_inconsistent_and_higher_index_systems_raise():
         create_ODE_system(["dx = -z - w", "0 = z**3 - x"], states={"x": 1.0, "z": 0.0, "w": 0.0})
     with pytest.raises(ExtraEquationsSystemError):
         create_ODE_system(["dx = -x", "0 = x**2 - 1"], states={"x": 1.0}, simplify=True)
-    # the pendulum in Cartesian coordinates is index 3: index reduction
-    # (Pantelides, dummy derivatives) is not built, and the input says so
-    with pytest.raises(InvalidSystemError, match="structurally singular"):
-        create_ODE_system("dx = vx\ndy = vy\ndvx = T*x\ndvy = T*y - g\n0 = x**2 + y**2 - L**2",
-                          states={"x": 1.0, "y": 0.0, "vx": 0.0, "vy": 0.0, "T": 0.0},
-                          constants={"g": 9.81, "L": 1.0})
+    # a constraint whose time derivative vanishes along the dynamics
+    # cannot be reduced (x + y is conserved: the system is redundant)
+    with pytest.raises(InvalidSystemError, match="vanishes identically"):
+        create_ODE_system(["dx = z", "dy = -z", "0 = x + y - 1"], states={"x": 0.5, "y": 0.5, "z": 0.0})
     with pytest.raises(InvalidSystemError, match="derivatives of algebraic unknowns"):
         create_ODE_system(["dx = -z", "0 = dz + x"], states={"x": 1.0, "z": 0.0})
     with pytest.raises(ValueError, match="immutable"):
@@ -223,3 +221,73 @@ def test_structural_helpers():
     assert _match([{x}, {x}], [x, y]) is None
     # 0 -> 1 -> 2 -> 1: components {1, 2} before {0}
     assert _components(3, [[1], [2], [1]]) == [[1, 2], [0]]
+
+
+PENDULUM = "dx = vx\ndy = vy\ndvx = T*x\ndvy = T*y - g\n0 = x**2 + y**2 - L**2"
+PENDULUM_STATES = {"x": 1.0, "y": 0.0, "vx": 0.0, "vy": 0.0, "T": 0.0}
+
+
+def test_pendulum_index_reduction_and_state_selection():
+    """The Cartesian pendulum (index 3): the constraint is differentiated
+    twice along the dynamics, its two lower derivatives stay as invariants
+    and demote one state each; with priorities on y and vy the solver
+    keeps y and vy, x stays as an algebraic state under x^2 + y^2 = L^2,
+    and vx and the tension T are solved for (observables)."""
+    sysm = create_ODE_system(PENDULUM, states=PENDULUM_STATES, constants={"g": 9.81, "L": 1.0},
+                             state_priority={"y": 10, "vy": 10}, precision=np.float64)
+    assert sysm.state_names == ["y", "vy", "x"]
+    assert [sysm.mass[i, i] for i in range(3)] == [1, 1, 0]
+    assert {"vx", "T"} <= set(sysm.observable_names)
+    x, y, vy = _s("x"), _s("y"), _s("vy")
+    assert sp.simplify(_deriv(sysm, "x") - (x**2 + y**2 - _s("L") ** 2)) == 0
+    assert sp.simplify(_obs(sysm, "vx") + vy * y / x) == 0
+    with pytest.raises(ValueError, match="implicit algorithm"):
+        Solver(sysm, algorithm="dormand-prince-54")
+    # without priorities the later-declared states are demoted
+    plain = create_ODE_system(PENDULUM, states=PENDULUM_STATES, constants={"g": 9.81, "L": 1.0})
+    assert plain.state_names == ["x", "vx", "y"] and {"vy", "T"} <= set(plain.observable_names)
+
+
+def _pendulum_reference(ts):
+    """Minimal coordinates: x = cos(phi), y = -sin(phi), phi'' = g cos(phi)."""
+    from scipy.integrate import solve_ivp as scipy_ivp
+    ref = scipy_ivp(lambda t, z: [z[1], 9.81 * np.cos(z[0])], (0.0, float(ts[-1])), [0.0, 0.0], rtol=1e-12,
+                    atol=1e-12, dense_output=True)
+    phi, dphi = ref.sol(ts)
+    return -np.sin(phi), -np.cos(phi) * dphi, np.cos(phi)
+
+
+def _pendulum_solver():
+    sysm = create_ODE_system(PENDULUM, states=PENDULUM_STATES, constants={"g": 9.81, "L": 1.0},
+                             state_priority={"y": 10, "vy": 10}, precision=np.float64)
+    return sysm, Solver(sysm, algorithm="radau", rtol=1e-10, atol=1e-10, linear_correction_type="direct",
+                        output_types=["state", "time"], save_every=0.05, dt_min=1e-14)
+
+
+def test_pendulum_solution_emulated():
+    """The index-reduced pendulum through the generated kernel (host build),
+    Radau IIA5, over t in [0, 0.3] (x stays away from 0, where the static
+    selection would turn singular): positions and velocity within 1e-8 of
+    the minimal-coordinates solution, the constraint held to rounding."""
+    from host_emu.emu import run_emulated
+    sysm, solver = _pendulum_solver()
+    x0 = np.array([[sysm.initial_values[n]] for n in sysm.state_names])
+    out = run_emulated(solver, x0, np.zeros((0, 1)), 0.3)
+    assert out["status"].tolist() == [0]
+    st = out["state"][:, :, 0]
+    y_ref, vy_ref, x_ref = _pendulum_reference(st[:, -1])
+    assert np.max(np.abs(st[:, 0] - y_ref)) < 1e-8 and np.max(np.abs(st[:, 1] - vy_ref)) < 1e-8
+    assert np.max(np.abs(st[:, 2] - x_ref)) < 1e-8
+    assert np.max(np.abs(st[:, 2] ** 2 + st[:, 0] ** 2 - 1.0)) < 1e-12
+
+
+@pytest.mark.gpu
+def test_pendulum_solution_gpu(cuda_device):
+    sysm, solver = _pendulum_solver()
+    x0 = np.array([[sysm.initial_values[n]] for n in sysm.state_names])
+    r = solver.solve(x0, np.zeros((0, 1)), duration=0.3, nan_error_trajectories=False)
+    assert r.status_codes.tolist() == [0]
+    st = r.state[:, :, 0]
+    y_ref, vy_ref, x_ref = _pendulum_reference(st[:, -1])
+    assert np.max(np.abs(st[:, 0] - y_ref)) < 1e-8 and np.max(np.abs(st[:, 1] - vy_ref)) < 1e-8
+    assert np.max(np.abs(st[:, 2] ** 2 + st[:, 0] ** 2 - 1.0)) < 1e-12
